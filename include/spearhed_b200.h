@@ -1,0 +1,242 @@
+/* spearhed_b200 — C ABI for the B200-native SPH(-MHD) step.
+ *
+ * The step this library replaces is spearHED's neighbour-region SPH step as
+ * composed by Simulation::runOneStep (include/spearhed/control/Simulation.x.cpp:196-310):
+ * drift -> neighbour search -> UpdateDensity -> UpdateHydroForces -> EulerIntegrate.
+ * It adds the terms the north-star step needs on top of the reference's
+ * inviscid hydro: artificial viscosity, SPMHD induction and magnetic stress,
+ * Dedner divergence cleaning, a CFL time step and FP64 conserved-quantity sums.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (SPH_OK == 0).  No C++ exception
+ *    crosses this boundary.  sph_last_error_string() describes the last failure
+ *    on the calling thread.
+ *  - Host arrays are caller-owned and are copied in (sph_set_species) and out
+ *    (sph_get_species).  Device memory is owned by the context.  Each context
+ *    owns one CUDA stream; a context is not thread-safe, distinct contexts on
+ *    distinct threads are.
+ *  - All host columns are FP64 ("double"), one array per attribute component
+ *    (structure of arrays), named after the reference's attribute tags
+ *    (include/spearhed/param/speciesDefinition.param:100-110): position, vel,
+ *    mass, smoothingLength (h), density, internalEnergy (u), dvdt, dudt, plus
+ *    the MHD columns B, psi, dBdt, dpsidt that the reference does not carry.
+ */
+#ifndef SPEARHED_B200_H
+#define SPEARHED_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum
+{
+    SPH_OK = 0,
+    SPH_ERR_INVALID = 1,       /* bad argument (null pointer, bad enum, n < 0 ...)          */
+    SPH_ERR_CUDA = 2,          /* a CUDA runtime call failed                                */
+    SPH_ERR_NOMEM = 3,         /* device allocation failed                                  */
+    SPH_ERR_OUTSIDE = 4,       /* a particle left a non-periodic box                        */
+    SPH_ERR_NONFINITE = 5,     /* NaN/Inf position, h <= 0 or mass <= 0 in the input        */
+    SPH_ERR_OVERFLOW = 6,      /* a neighbour list exceeded its capacity (retry is automatic) */
+    SPH_ERR_STATE = 7,         /* call out of order (e.g. hydro before density)             */
+    SPH_ERR_TIMEOUT = 8,       /* a bounded wait on the device gave up                      */
+    SPH_ERR_UNSUPPORTED = 9    /* configuration this build does not implement               */
+};
+
+/* ---- kernels (SphKernel models, include/spearhed/sph/SphKernel.hpp:45-51) -- */
+enum
+{
+    SPH_KERNEL_CUBIC = 0,      /* M4 cubic spline, support 2h (CubicSplineKernel.hpp:40)      */
+    SPH_KERNEL_QUINTIC = 1,    /* M5 quintic spline, support 3h (QuinticSplineKernel.hpp:39)  */
+    SPH_KERNEL_WENDLAND_C2 = 2 /* Wendland C2, support 2h (not in the reference)              */
+};
+
+/* ---- physics switches (SphParams.physics bit mask) --------------------- */
+enum
+{
+    SPH_PHYS_AV = 1u << 0,       /* Monaghan artificial viscosity (alpha, beta)              */
+    SPH_PHYS_MHD = 1u << 1,      /* SPMHD induction + Maxwell stress                         */
+    SPH_PHYS_DEDNER = 1u << 2,   /* Dedner/Tricco-Price hyperbolic divergence cleaning       */
+    SPH_PHYS_TENSILE = 1u << 3,  /* Borve tensile-instability correction of the stress       */
+    SPH_PHYS_CFL = 1u << 4       /* adaptive dt from the CFL/force criteria (FP64 min)       */
+};
+
+/* ---- precision of the pair kernels -------------------------------------- */
+enum
+{
+    SPH_PREC_FP64 = 0,         /* FP64 plain pair kernels                                    */
+    SPH_PREC_FP32_COMP = 1     /* FP32 pair kernels with compensated (two-sum) accumulation  */
+};
+
+/* ---- neighbour acceptance radius ---------------------------------------- */
+enum
+{
+    SPH_CULL_GLOBAL = 0,       /* r^2 < (support*h0)^2: the reference's interact() radius    */
+    SPH_CULL_PAIR_MAX = 1      /* r^2 < (support*max(h_i,h_j))^2: variable h                 */
+};
+
+/* ---- species and roles (include/spearhed/param/speciesDefinition.param:56-88,
+ *      spmacc/particles/regions/RegionRole.hpp:42-62) ---------------------- */
+enum
+{
+    SPH_SPECIES_DEFAULT = 0,   /* Interior|Movable|Source|Thermodynamic */
+    SPH_SPECIES_BOUNDARY = 1,  /* Frozen|Source|Thermodynamic           */
+    SPH_SPECIES_TRACER = 2,    /* Movable                               */
+    SPH_NUM_SPECIES = 3
+};
+enum
+{
+    SPH_ROLE_MOVABLE = 1u << 0,
+    SPH_ROLE_SOURCE = 1u << 1,
+    SPH_ROLE_THERMODYNAMIC = 1u << 2,
+    SPH_ROLE_FROZEN = 1u << 3,
+    SPH_ROLE_INTERIOR = 1u << 4
+};
+#define SPH_ROLES_DEFAULT (SPH_ROLE_INTERIOR | SPH_ROLE_MOVABLE | SPH_ROLE_SOURCE | SPH_ROLE_THERMODYNAMIC)
+#define SPH_ROLES_BOUNDARY (SPH_ROLE_FROZEN | SPH_ROLE_SOURCE | SPH_ROLE_THERMODYNAMIC)
+#define SPH_ROLES_TRACER (SPH_ROLE_MOVABLE)
+
+/* ---- run-time parameters (replace the reference's compile-time .param
+ *      files: include/spearhed/param/sph.param:26-34, dimension.param:28-35) */
+typedef struct SphParams
+{
+    int32_t kernel;        /* SPH_KERNEL_*                                                  */
+    int32_t precision;     /* SPH_PREC_*                                                    */
+    int32_t cull;          /* SPH_CULL_*                                                    */
+    uint32_t physics;      /* SPH_PHYS_* mask; 0 = the reference's inviscid hydro           */
+    double gamma;          /* adiabatic index (gamma_eos)                                   */
+    double h0;             /* smoothing length used for the global cull radius (h0)         */
+    double dt;             /* fixed time step, or the first step's dt when SPH_PHYS_CFL      */
+    double alpha, beta;    /* artificial viscosity (Monaghan 1992), e.g. 1 and 2             */
+    double av_eps;         /* eta^2 regulariser in mu_ij, 0.01                              */
+    double cfl;            /* Courant factor for SPH_PHYS_CFL, e.g. 0.3                      */
+    double cfl_force;      /* factor of the force criterion sqrt(h/|a|), e.g. 0.25          */
+    double dedner_sigma;   /* Dedner damping constant sigma (tau = h/(sigma c_h)), e.g. 1    */
+    double mu0;            /* magnetic permeability in code units (1)                        */
+    int32_t max_neighbours;/* per-particle neighbour-list capacity; 0 = library default      */
+    int32_t device;        /* CUDA device ordinal                                           */
+} SphParams;
+
+/* A particle box: the reference's fluid/wall domain (an AABB, spmacc/particles/regions/AABB.hpp:38-127).
+ * Particles must stay inside [lo, hi) along non-periodic axes. */
+typedef struct SphBox
+{
+    double lo[3];
+    double hi[3];
+    int32_t periodic[3];
+} SphBox;
+
+/* Column pointers for one species (host, FP64, length n).  Any pointer may be
+ * NULL: on input the attribute is then zero (h defaults to params.h0); on
+ * output it is skipped.  box_id (int32) selects the ensemble box (NULL = 0). */
+typedef struct SphSoAView
+{
+    double* pos[3];
+    double* vel[3];
+    double* mass;
+    double* h;
+    double* density;
+    double* u;
+    double* dvdt[3];
+    double* dudt;
+    double* B[3];
+    double* psi;
+    double* dBdt[3];
+    double* dpsidt;
+    double* divB;
+    int32_t* box_id;
+} SphSoAView;
+
+/* Conserved quantities and step diagnostics, FP64 sums over the
+ * Movable & Thermodynamic particles (block-then-grid reductions on the device). */
+typedef struct SphDiag
+{
+    double time;           /* simulated time                                                */
+    double dt;             /* dt of the last step                                           */
+    double dt_next;        /* dt the next step will use                                     */
+    double e_kin;          /* sum 1/2 m v^2                                                 */
+    double e_int;          /* sum m u                                                       */
+    double e_mag;          /* sum 1/2 m B^2 / (mu0 rho)                                     */
+    double mom[3];         /* sum m v                                                       */
+    double divb_mean;      /* mean of |divB| h / |B| (|B| > 0)                              */
+    double divb_max;       /* max of |divB| h / |B|                                         */
+    double c_h;            /* Dedner cleaning speed of the last force pass                  */
+    double pairs;          /* ordered accepted pairs (i != j) of the last neighbour build   */
+    int64_t steps;         /* steps taken by this context                                   */
+    int64_t n_targets;     /* particles in the sums                                         */
+} SphDiag;
+
+typedef struct sph_ctx sph_ctx;
+
+/* Fill *p with the library defaults (cubic kernel, FP32-compensated, global
+ * cull, inviscid hydro, gamma 5/3, h0 0.05, dt 0.01 — the reference's param files). */
+int sph_default_params(SphParams* p);
+
+/* Replaces: Simulation::init / pluginLoad device and heap setup
+ * (include/spearhed/control/Simulation.x.cpp:129-169, 312-352). */
+int sph_create(const SphParams* params, sph_ctx** out);
+int sph_destroy(sph_ctx* ctx);
+
+/* Replaces: the setup's domain AABB and region list
+ * (share/spearhed/ValidationSetups/SodShockTube.hpp:442-467, InitRegions.hpp:47-104).
+ * nbox > 1 makes an ensemble of independent boxes (particles select theirs by box_id). */
+int sph_set_boxes(sph_ctx* ctx, int32_t nbox, const SphBox* boxes);
+
+/* Replaces: InitParticles filling a species' ParticleRegionBuffer
+ * (include/spearhed/particles/initialization/InitParticles.hpp:284-433). */
+int sph_set_species(sph_ctx* ctx, int32_t species_id, uint32_t roles, int64_t n, const SphSoAView* view);
+
+/* Replaces: ParticleRegionBuffer::deviceToHost + frame iteration in the tests
+ * (tests/spearhed/unit/DensitySummation/DensitySummation.cpp:258-276).  Copies the
+ * species back in the order it was given to sph_set_species. */
+int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* view);
+
+/* Replaces: UpdateDensity<K>{}(bundle, target, index, h0)
+ * (include/spearhed/particles/density/DensitySummation.hpp:104-138), including the
+ * neighbour search it relies on (calculateNeighboursSender, NeighbourRegions.hpp:233-255). */
+int sph_density(sph_ctx* ctx);
+
+/* Replaces: UpdateHydroForces<K>{gamma}(bundle, target, index, h0)
+ * (include/spearhed/sph/HydroForces.hpp:183-214).  Uses the density of the last
+ * sph_density call.  With SPH_PHYS_AV the viscosity terms are added. */
+int sph_hydro(sph_ctx* ctx);
+
+/* The SPMHD pass (induction, Maxwell stress, Dedner): no reference counterpart.
+ * Runs the full force pass with the MHD terms enabled in params.physics. */
+int sph_mhd(sph_ctx* ctx);
+
+/* Replaces: Simulation::runOneStep repeated n_steps times
+ * (include/spearhed/control/Simulation.x.cpp:196-310): drift, neighbour search,
+ * density, forces, kick.  dt > 0 overrides params.dt for these steps; dt <= 0
+ * keeps params.dt (or the CFL dt when SPH_PHYS_CFL is set). */
+int sph_step(sph_ctx* ctx, int32_t n_steps, double dt);
+
+/* Conserved-quantity reductions of the current state (no reference counterpart;
+ * PMacc's device::Reduce, packages/pmacc/include/pmacc/device/Reduce.hpp:41, is unused there). */
+int sph_reduce(sph_ctx* ctx, SphDiag* out);
+
+/* Per-box diagnostics of an ensemble: out[nbox]. */
+int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out);
+
+/* Per-particle accepted-neighbour counts (i != j) of the last neighbour build, for
+ * one species in its input order (int32, length n).  Used to prove that the
+ * accepted pair set equals the oracle's. */
+int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts);
+
+/* Device time of the last sph_step / sph_density / sph_hydro call per stage,
+ * in milliseconds: [0] sort+permute, [1] density, [2] force, [3] integrate+reduce,
+ * [4] whole call.  n is the array length (<= 5). */
+int sph_get_timings(sph_ctx* ctx, int32_t n, double* ms);
+
+/* Capture each later sph_step's per-step launch sequence in a CUDA graph and
+ * replay it (on = 1) or launch the kernels one by one (on = 0, the default). */
+int sph_use_graph(sph_ctx* ctx, int32_t on);
+
+const char* sph_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPEARHED_B200_H */

@@ -1,0 +1,3 @@
+/* Declarations only (see spmacc/particles/algorithms/InteractParticles.hpp here). */
+#pragma once
+#include <spmacc/particles/algorithms/InteractParticles.hpp>

@@ -1,0 +1,140 @@
+"""Host-side initial conditions for the benchmark and test workloads.
+
+These play the part of the reference's setup blocks (SetupInterface +
+InitParticles + the SC lattice: include/spearhed/particles/initialization/
+InitParticles.hpp:284-433, spmacc/particles/initialization/SC.hpp:118-200,
+share/spearhed/ValidationSetups/SodShockTube.hpp:128-176): they place particles
+on simple-cubic lattices at cell centres, with equal masses, u = P/((gamma-1) rho).
+Jitter, where a workload asks for it, comes from numpy's Philox4x32-10
+counter-based generator keyed by the workload's seed.
+
+Each generator returns a :class:`Workload`.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import abi
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    params: abi.SphParams
+    boxes: list
+    species: dict  # species id -> abi.Species
+    steps: int = 1
+    meta: dict = dataclasses.field(default_factory=dict)
+
+    @property
+    def n(self):
+        return sum(s.n for s in self.species.values())
+
+    def combined(self):
+        """All species concatenated (Default, Boundary, Tracer order) with their roles."""
+        parts, roles = [], []
+        for sid in sorted(self.species):
+            s = self.species[sid]
+            parts.append(s)
+            roles.append(np.full(s.n, abi.SPECIES_ROLES[sid], dtype=np.uint8))
+        return abi.Species.concat(parts), np.concatenate(roles)
+
+    def split(self, combined):
+        """Inverse of :meth:`combined` for a state array set of the same layout."""
+        out, off = {}, 0
+        for sid in sorted(self.species):
+            n = self.species[sid].n
+            s = abi.Species(n)
+            for c in abi.COLUMNS:
+                setattr(s, c, np.ascontiguousarray(getattr(combined, c)[..., off:off + n]))
+            s.box_id = np.ascontiguousarray(combined.box_id[off:off + n])
+            out[sid] = s
+            off += n
+        return out
+
+
+def lattice(lo, hi, counts):
+    """Simple-cubic lattice at cell centres of the box lo..hi (SC.hpp:118-200)."""
+    axes = [lo[a] + (np.arange(counts[a]) + 0.5) * (hi[a] - lo[a]) / counts[a] for a in range(3)]
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()])
+
+
+def philox_uniform(seed, shape):
+    return np.random.Generator(np.random.Philox(key=seed)).uniform(-1.0, 1.0, size=shape)
+
+
+def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False):
+    """3D Sod shock tube, gamma 1.4, periodic in y and z.
+
+    Left x in [-0.5, 0): rho 1, P 1 on a (64 s)x(16 s)x(16 s) lattice; right
+    x in [0, 0.5): rho 0.125, P 0.1 on (32 s)x(8 s)x(8 s); s = ``scale`` (1 gives
+    N = 18432).  Equal masses; h = 1.2 x local spacing (56 lattice neighbours);
+    cubic spline; artificial viscosity alpha 1, beta 2; CFL 0.3.  x is open: the
+    box extends 0.25 beyond each end.  ``scale`` < 1 is allowed as a fraction
+    (e.g. 0.5 halves every lattice count).
+    """
+    gamma = 1.4
+    nl = (int(64 * scale), int(16 * scale), int(16 * scale))
+    nr = (int(32 * scale), int(8 * scale), int(8 * scale))
+    Ly = 0.125
+    left = lattice((-0.5, 0.0, 0.0), (0.0, Ly, Ly), nl)
+    right = lattice((0.0, 0.0, 0.0), (0.5, Ly, Ly), nr)
+    dxl, dxr = 0.5 / nl[0], 0.5 / nr[0]
+    m = 1.0 * dxl ** 3
+    n = left.shape[1] + right.shape[1]
+    s = abi.Species(n)
+    s.pos[:] = np.concatenate([left, right], axis=1)
+    s.mass[:] = m
+    s.h[:] = np.concatenate([np.full(left.shape[1], 1.2 * dxl), np.full(right.shape[1], 1.2 * dxr)])
+    rho = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.125)])
+    P = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.1)])
+    s.density[:] = rho
+    s.u[:] = P / ((gamma - 1.0) * rho)
+    physics = 0 if reference_physics else (abi.PHYS_AV | abi.PHYS_CFL)
+    params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                physics=physics, gamma=gamma, h0=1.2 * dxr, dt=1e-4, alpha=1.0, beta=2.0,
+                                cfl=0.3)
+    box = abi.make_box((-0.75, 0.0, 0.0), (0.75, Ly, Ly), (0, 1, 1))
+    return Workload("sod_small", params, [box], {abi.SPECIES_DEFAULT: s}, steps=50,
+                    meta={"n_left": left.shape[1], "n_right": right.shape[1], "dx_left": dxl, "dx_right": dxr})
+
+
+def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45):
+    """Orszag-Tang vortex in a thin periodic slab [0,1]^2 x [0, nz/nx].
+
+    nx x nx x nz lattice of equal-mass particles; rho = 25/(36 pi), P = 5/(12 pi),
+    gamma = 5/3, v = (-sin 2 pi y, sin 2 pi x, 0), B = (-sin 2 pi y, sin 4 pi x, 0)/sqrt(4 pi).
+    Wendland C2 with h = hfact x spacing (hfact 1.45: 92 lattice neighbours,
+    ~102 in the continuum), AV, SPMHD with Dedner cleaning and the tensile
+    correction, CFL time step.  nx = 512, nz = 4 gives N = 1,048,576.
+    """
+    gamma = 5.0 / 3.0
+    dx = 1.0 / nx
+    Lz = nz * dx
+    pos = lattice((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (nx, nx, nz))
+    n = pos.shape[1]
+    s = abi.Species(n)
+    s.pos[:] = pos
+    rho0 = 25.0 / (36.0 * math.pi)
+    P0 = 5.0 / (12.0 * math.pi)
+    s.mass[:] = rho0 * dx ** 3
+    s.h[:] = hfact * dx
+    s.density[:] = rho0
+    s.u[:] = P0 / ((gamma - 1.0) * rho0)
+    x, y = pos[0], pos[1]
+    s.vel[0] = -np.sin(2 * math.pi * y)
+    s.vel[1] = np.sin(2 * math.pi * x)
+    b0 = 1.0 / math.sqrt(4 * math.pi)
+    s.B[0] = -b0 * np.sin(2 * math.pi * y)
+    s.B[1] = b0 * np.sin(4 * math.pi * x)
+    physics = abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
+    params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_GLOBAL,
+                                physics=physics, gamma=gamma, h0=hfact * dx, dt=2e-4, alpha=1.0, beta=2.0,
+                                cfl=0.3, dedner_sigma=1.0)
+    box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (1, 1, 1))
+    return Workload("orszag_tang", params, [box], {abi.SPECIES_DEFAULT: s}, steps=200,
+                    meta={"nx": nx, "nz": nz, "dx": dx})
