@@ -1,0 +1,391 @@
+"""Benchmark: SPH pair-interactions/s of the Orszag-Tang SPMHD step on B200.
+
+Workload (default): Orszag-Tang vortex, thin periodic slab [0,1]^2 x [0,1/128],
+512 x 512 x 4 lattice = 1,048,576 equal-mass particles, Wendland C2 kernel
+(h = 1.45 spacing, ~100 neighbours), artificial viscosity, SPMHD with Dedner
+cleaning and the tensile correction, CFL time step; synthetic initial
+conditions of that shape (no dataset is involved).
+
+A step is one full runOneStep: drift, cell keys, radix sort, permute, neighbour
+build + density, fused hydro/AV + SPMHD/Dedner force pass, kick, FP64
+conserved-quantity reductions and the CFL minimum.
+
+value  = accepted ordered pairs per pass x 3 logical pair passes (density,
+         hydro/AV, SPMHD/Dedner) per step x steps / device time of those steps
+         (CUDA events on the library's stream), FP32-compensated pair kernels.
+e2e    = the same metric through the C ABI with pinned host buffers: every
+         step copies the state in (sph_set_species), runs sph_step(1) and copies
+         the state out (sph_get_species), all inside the timed region.
+The FP64-plain kernel on the same GPU and workload is reported beside it
+(fp64_plain), with the FP32 run's errors against it after one step.
+
+--impl reference times the reference's own CPU path for this step (its density
+and hydro functors compiled from the reference sources, oracle/_ref, driven by
+a restatement of its region/frame pair engine) on the host cores, or the
+oracle port when oracle/_ref is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SPH pair-interactions/s: FP32-mixed vs FP64 plain on 1 B200 at stated error"
+UNIT = "pair-interactions/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--fp64-steps", type=int, default=5)
+    ap.add_argument("--graph", action="store_true", help="replay the step as a CUDA graph")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[4 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- helpers
+def pinned_species(src, fields):
+    """A Species whose listed columns live in pinned host memory (torch)."""
+    import torch
+
+    from spearhed_b200 import abi
+    s = abi.Species(src.n)
+    for f in fields:
+        a = getattr(src, f)
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        arr = t.numpy()
+        arr[...] = a
+        setattr(s, f, arr)
+        s.__dict__.setdefault("_pins", []).append(t)
+    return s
+
+
+def traffic_from_profiles(name):
+    """DRAM bytes per launch recorded from an ncu capture under profiles/ (or None)."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_full_workload:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak(key):
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get(key)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------- CPU baselines
+def cpu_reference_sample(nx, nz, budget_s=20.0):
+    """The reference's density + hydro functors (compiled from its sources) over
+    a sample of target frames of the same workload, driven by its region/frame
+    engine restated in oracle/ref_functors.cpp.  Falls back to the oracle port."""
+    from oracle import pyoracle
+    from spearhed_b200 import abi, setups
+    w = setups.orszag_tang(nx=nx, nz=nz)
+    s = w.species[abi.SPECIES_DEFAULT]
+    cores = os.cpu_count() or 1
+    ref = pyoracle.ref()
+    if ref is not None and hasattr(ref, "ref_region_bench_f32"):
+        box = w.boxes[0]
+        side = 4.0 / nx  # regions of 4 x 4 x 4 lattice cells = one 64-slot frame each
+        r = pyoracle.region_bench(s, w.params, list(box.lo), list(box.hi), side, budget_s=budget_s)
+        r["cores"] = cores
+        return r
+    # Oracle port: density + force of the full SPMHD step on a smaller slab of
+    # the same resolution (nx_sample^2 x nz), all host threads.
+    nxs = 128
+    ws = setups.orszag_tang(nx=nxs, nz=nz)
+    ss = ws.species[abi.SPECIES_DEFAULT].copy()
+    ws.params.precision = abi.PREC_FP64
+    orc = pyoracle.System(ws.params, ws.boxes, ss, np.full(ss.n, abi.ROLES_DEFAULT, dtype=np.uint8))
+    _, pairs = orc.neighbour_counts()
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.density()
+        orc.force()
+        reps += 1
+        if time.perf_counter() - t0 > min(budget_s, 10.0):
+            break
+    dt = time.perf_counter() - t0
+    return {"value": 3 * pairs * reps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle FP64 density + SPMHD force passes ({reps} reps) on a {nxs}x{nxs}x{nz} slab of the "
+                      f"same spacing ({ss.n} particles), 3 logical pair passes per accepted pair"}
+
+
+# ------------------------------------------------------------------ main
+def run_ours(args, rank, world):
+    import torch
+
+    import spearhed_b200 as sb
+    from spearhed_b200 import abi, flops, setups
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    L = abi.lib()
+    L.sphx_fma_tflops.restype = C.c_int
+    L.sphx_fma_tflops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.sphx_launch_count.restype = C.c_ulonglong
+
+    w = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
+    w.params.device = dev
+    n = w.n
+    ctx = sb.context_for(w)
+    if args.graph:
+        ctx.use_graph(True)
+    ctx.step(args.warmup)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    d0 = ctx.reduce()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = L.sphx_launch_count()
+    with ClockSampler(dev) as clk:
+        ctx.step(args.steps)
+        torch.cuda.synchronize()
+    launches = L.sphx_launch_count() - launches0
+    barrier()
+    tm = ctx.timings()  # [build, density, force, kick, whole] ms over the timed steps
+    d1 = ctx.reduce()
+    pairs = d1["pairs_total"] - d0["pairs_total"]
+    ms_total = tm[4]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_total, pairs], dtype=torch.float64, device=f"cuda:{dev}")
+        mx = t.clone()
+        dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+        ms_total, pairs = float(mx[0]), float(t[1])
+    passes = flops.PASSES_PER_STEP["mhd"]
+    value = passes * pairs / (ms_total * 1e-3)
+    ms_step = ms_total / args.steps
+
+    # roofline of the dominant kernel (the fused force pass), FP32 FMA pipe
+    pairs_step = pairs / args.steps / max(world, 1)
+    force_ms = tm[2] / args.steps
+    dens_ms = tm[1] / args.steps
+    peak = C.c_double(0)
+    L.sphx_fma_tflops(dev, 0, C.byref(peak))
+    peak64 = C.c_double(0)
+    L.sphx_fma_tflops(dev, 1, C.byref(peak64))
+    force_flops = flops.FORCE_FLOPS["mhd"] * pairs_step
+    achieved = force_flops / (force_ms * 1e-3) / 1e12
+    dens_achieved = flops.DENSITY_FLOPS["wendland_c2"] * pairs_step / (dens_ms * 1e-3) / 1e12
+    traffic = traffic_from_profiles("force_mhd_fp32_orszag_tang.txt")
+    result = {}
+    if rank == 0:
+        # ---- FP64 plain, same workload, same GPU
+        w64 = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP64)
+        w64.params.device = dev
+        ctx64 = sb.context_for(w64)
+        ctx64.step(args.warmup)
+        e0 = ctx64.reduce()
+        ctx64.step(args.fp64_steps)
+        t64 = ctx64.timings()
+        e1 = ctx64.reduce()
+        v64 = passes * (e1["pairs_total"] - e0["pairs_total"]) / (t64[4] * 1e-3)
+        ctx64.close()
+        # ---- errors of the FP32 step against the FP64 step from the same state
+        wa = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
+        wb = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP64)
+        ca, cb = sb.context_for(wa), sb.context_for(wb)
+        ca.step(1)
+        cb.step(1)
+        ga, gb = ca.get_species(0), cb.get_species(0)
+        err_rho = float(np.max(np.abs(ga.density / gb.density - 1.0)))
+        err_acc = float(np.max(np.abs(ga.dvdt - gb.dvdt)) / np.max(np.abs(gb.dvdt)))
+        err_dB = float(np.max(np.abs(ga.dBdt - gb.dBdt)) / np.max(np.abs(gb.dBdt)))
+        ca.close()
+        cb.close()
+        # ---- end to end through the C ABI with pinned host buffers
+        wi = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
+        cols_in = ["pos", "vel", "mass", "h", "density", "u", "B", "psi"]
+        cols_out = ["pos", "vel", "density", "u", "B", "psi"]
+        host = pinned_species(wi.species[0], cols_in)
+        out = pinned_species(wi.species[0], cols_out)
+        ce = sb.Context(wi.params, wi.boxes)
+        ce.set_species(0, host)
+        ce.step(1)
+        ce.get_species(0)  # allocations + list sizing happen here, outside timing
+        L.sph_get_species.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.SphSoAView)]
+        vin, vout = host.view(), out.view()
+        for f in ("dvdt", "dudt", "dBdt", "dpsidt", "divB"):
+            if f in abi.VECTOR_COLUMNS:
+                for a in range(3):
+                    getattr(vout, f)[a] = None
+            else:
+                setattr(vout, f, None)
+        for f in ("mass", "h"):
+            setattr(vout, f, None)
+        vout.box_id = None
+        pe0 = ce.reduce()["pairs_total"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            abi.check(L.sph_set_species(ce._p, 0, abi.ROLES_DEFAULT, host.n, C.byref(vin)))
+            abi.check(L.sph_step(ce._p, 1, 0.0))
+            abi.check(L.sph_get_species(ce._p, 0, C.byref(vout)))
+            host.pos[...] = out.pos  # the next step starts from this step's result
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        pe1 = ce.reduce()["pairs_total"]
+        ce.close()
+        e2e_pairs = (pe1 - pe0) / args.e2e_steps
+        h2d = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_in) * 8 * n
+        d2h = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_out) * 8 * n
+        # ---- CPU baseline (rank 0, N = 1 only)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_reference_sample(args.nx, args.nz)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair kernels (compensated), fp64 integration",
+            "data": "synthetic Orszag-Tang initial conditions (lattice, analytic v and B)",
+            "config": {"workload": "orszag_tang_slab_512x512x4", "particles": n, "kernel": "wendland_c2",
+                       "h_over_dx": 1.45, "neighbours_mean": pairs_step / n, "physics": "hydro+AV+SPMHD+Dedner+CFL",
+                       "pair_passes_per_step": passes, "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "working set > L2 (lists ~" + f"{n * 4 * 136 / 1e9:.2f}" + " GB, state ~0.3 GB)",
+                       "graph": bool(args.graph)},
+            "stage_ms_per_step": {"sort_permute": tm[0] / args.steps, "density": dens_ms, "force": force_ms,
+                                  "kick_reduce": tm[3] / args.steps},
+            "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": t64[4] / args.fp64_steps,
+                           "fp32_speedup": value / v64 if v64 else None},
+            "error_vs_fp64_after_1_step": {"density_rel_max": err_rho, "accel_normwise": err_acc,
+                                           "dBdt_normwise": err_dB},
+            "roofline": {"bound": "fp32_fma", "kernel": "kForce<WendlandC2,float,SPMHD>",
+                         "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
+                         "flops_per_pair": flops.FORCE_FLOPS["mhd"], "pairs_per_launch": pairs_step,
+                         "peak_source": "measured live (FMA-chain microbenchmark, sphx_fma_tflops)",
+                         "density_kernel": {"achieved": dens_achieved, "flops_per_pair": flops.DENSITY_FLOPS["wendland_c2"]},
+                         "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs")},
+            "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            result["cpu_baseline"] = cpu
+    ctx.close()
+    return result
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cpu = cpu_reference_sample(args.nx, args.nz, budget_s=max(5.0, 2.0 * args.steps))
+        line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp32" if cpu.get("kind") == "reference" else "fp64",
+                "data": "synthetic Orszag-Tang initial conditions",
+                "config": {"workload": "orszag_tang_slab_512x512x4"}, "impl": "reference",
+                "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                             "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_ours(args, rank, world)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -166,6 +166,7 @@ typedef struct SphDiag
     double pairs;          /* ordered accepted pairs (i != j) of the last neighbour build   */
     int64_t steps;         /* steps taken by this context                                   */
     int64_t n_targets;     /* particles in the sums                                         */
+    double pairs_total;    /* accepted ordered pairs summed over every step's neighbour build */
 } SphDiag;
 
 typedef struct sph_ctx sph_ctx;

@@ -94,6 +94,11 @@ def ref():
             f.restype = None
             f.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), TP, TP, TP, C.POINTER(C.c_int64),
                           C.POINTER(C.c_int), TP, T, TP]
+            f = getattr(L, f"ref_region_bench_{suf}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, C.c_int, TP, TP, TP, TP, TP, TP, TP, TP, T, T, T, C.c_double,
+                          C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                          C.POINTER(C.c_double)]
             f = getattr(L, f"ref_hydro_{suf}")
             f.restype = None
             f.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), TP, TP, TP, TP, TP, TP, C.POINTER(C.c_int64),
@@ -190,3 +195,39 @@ class System:
 def _check(st):
     if st != 0:
         raise RuntimeError(f"oracle error {st}")
+
+
+def region_bench(species, params, box_lo, box_hi, side, budget_s=20.0, dtype=np.float32):
+    """Time the reference's density + hydro functors (compiled from its sources)
+    under its region/frame engine on the host cores: regions of edge `side`,
+    64-slot frames, cubic spline with the radius 2*h0 of `params`.  Target
+    frames run in order until `budget_s` has passed.  Returns a cpu_baseline dict."""
+    L = ref()
+    T = C.c_float if dtype == np.float32 else C.c_double
+    suf = "f32" if dtype == np.float32 else "f64"
+    n = species.n
+
+    def arr(a):
+        return np.ascontiguousarray(a, dtype=dtype)
+    pos = arr(species.pos.T.ravel())
+    vel = arr(species.vel.T.ravel())
+    mass, h, u = arr(species.mass), arr(species.h), arr(species.u)
+    rho = arr(species.density).copy()
+    lo, hi = arr(box_lo), arr(box_hi)
+    P = lambda a: a.ctypes.data_as(C.POINTER(T))  # noqa: E731
+    pd, ph = C.c_int64(0), C.c_int64(0)
+    fd, ft = C.c_int(0), C.c_int(0)
+    sec = C.c_double(0)
+    st = getattr(L, f"ref_region_bench_{suf}")(
+        0, n, P(pos), P(mass), P(h), P(rho), P(u), P(vel), P(lo), P(hi), side, 2.0 * params.h0, params.gamma,
+        budget_s, C.byref(pd), C.byref(ph), C.byref(fd), C.byref(ft), C.byref(sec))
+    _check(st)
+    value = (pd.value + ph.value) / sec.value
+    return {"value": value, "unit": "pair-interactions/s", "kind": "reference",
+            "pairs_density": pd.value, "pairs_hydro": ph.value, "seconds": sec.value,
+            "frames": [fd.value, ft.value],
+            "sample": (f"{fd.value} of {ft.value} target frames of the {n}-particle input: the reference's own "
+                       "DensityInitSelf/AccumulateDensity and HydroInteraction functors (compiled from its "
+                       "headers, FP32) under its region/frame engine (64-slot frames, AABB region search), "
+                       "cubic spline at the same 2h radius, no periodic images (the reference has none); "
+                       "2 pair passes (density, hydro)")}

@@ -100,6 +100,7 @@ class SphDiag(C.Structure):
         ("pairs", C.c_double),
         ("steps", C.c_int64),
         ("n_targets", C.c_int64),
+        ("pairs_total", C.c_double),
     ]
 
     def as_dict(self):

@@ -1,0 +1,1185 @@
+// Host runtime and C ABI of the B200 SPH step (include/spearhed_b200.h).
+//
+// One sph_ctx owns one CUDA stream and all device memory of a run.  A step is
+// a fixed sequence of launches on that stream with every scalar it needs (dt,
+// time, c_h, the CFL minimum) kept in device memory, so a step never waits for
+// the host and pairs of steps are captured into CUDA graphs on request.  This
+// takes the place of the reference's runOneStep sender graph and of its two
+// host round trips per step (NeighbourRegions.hpp:186-191, FrameIndex.hpp:209-280).
+//
+// Data flow: sph_set_species keeps a host mirror until the first compute call
+// allocates the device state; after that, a species of unchanged size is
+// copied straight from the caller's columns (pinned memory makes these copies
+// asynchronous) into a staging column and gathered into the sorted state.
+#include "sph_launch.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace
+{
+    thread_local std::string g_lastError;
+
+    int fail(int code, std::string msg)
+    {
+        g_lastError = std::move(msg);
+        return code;
+    }
+
+#define SPH_CUDA_TRY(expr)                                                                                             \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t const e_ = (expr);                                                                                 \
+        if(e_ != cudaSuccess)                                                                                          \
+            return fail(                                                                                               \
+                e_ == cudaErrorMemoryAllocation ? SPH_ERR_NOMEM : SPH_ERR_CUDA,                                        \
+                std::string(#expr) + ": " + cudaGetErrorString(e_));                                                   \
+    } while(0)
+
+    // Host columns of a species, in the order of the master state.
+    constexpr int kHostCols = 14;
+    enum
+    {
+        cX = 0,
+        cY,
+        cZ,
+        cVX,
+        cVY,
+        cVZ,
+        cU,
+        cM,
+        cH,
+        cRho,
+        cBX,
+        cBY,
+        cBZ,
+        cPsi
+    };
+
+    struct HostSpecies
+    {
+        bool set = false;
+        uint32_t roles = 0;
+        int64_t n = 0;
+        std::vector<double> col[kHostCols];
+        std::vector<int32_t> box;
+        uint32_t offset = 0;
+    };
+
+    int supportOf(int kernel)
+    {
+        return kernel == SPH_KERNEL_QUINTIC ? 3 : 2;
+    }
+
+    //! Smallest admissible cell edge for cull radius support*h: the larger of
+    //! the FP64 and FP32 radius, widened by 2^-20 (same rule as the oracle).
+    double cellRadius(int sup, double h)
+    {
+        double const r64 = double(sup) * h;
+        double const r32 = double(float(sup) * float(h));
+        return (r64 > r32 ? r64 : r32) * (1.0 + 1.0 / 1048576.0);
+    }
+
+    //! Input pointer of host column c in a view (nullptr when absent).
+    double const* viewCol(SphSoAView const* v, int c)
+    {
+        if(!v)
+            return nullptr;
+        switch(c)
+        {
+        case cX:
+        case cY:
+        case cZ:
+            return v->pos[c - cX];
+        case cVX:
+        case cVY:
+        case cVZ:
+            return v->vel[c - cVX];
+        case cU:
+            return v->u;
+        case cM:
+            return v->mass;
+        case cH:
+            return v->h;
+        case cRho:
+            return v->density;
+        case cBX:
+        case cBY:
+        case cBZ:
+            return v->B[c - cBX];
+        case cPsi:
+            return v->psi;
+        }
+        return nullptr;
+    }
+
+    int validateParams(SphParams const& p)
+    {
+        if(p.kernel < SPH_KERNEL_CUBIC || p.kernel > SPH_KERNEL_WENDLAND_C2)
+            return fail(SPH_ERR_INVALID, "unknown kernel");
+        if(p.precision != SPH_PREC_FP64 && p.precision != SPH_PREC_FP32_COMP)
+            return fail(SPH_ERR_INVALID, "unknown precision");
+        if(p.cull != SPH_CULL_GLOBAL && p.cull != SPH_CULL_PAIR_MAX)
+            return fail(SPH_ERR_INVALID, "unknown cull mode");
+        if(!(p.h0 > 0.0) || !std::isfinite(p.h0))
+            return fail(SPH_ERR_INVALID, "h0 must be positive");
+        if(!(p.gamma > 1.0))
+            return fail(SPH_ERR_INVALID, "gamma must be > 1");
+        if((p.physics & SPH_PHYS_DEDNER) && !(p.physics & SPH_PHYS_MHD))
+            return fail(SPH_ERR_INVALID, "Dedner cleaning needs SPH_PHYS_MHD");
+        if(p.max_neighbours < 0)
+            return fail(SPH_ERR_INVALID, "max_neighbours must be >= 0");
+        return SPH_OK;
+    }
+} // namespace
+
+struct sph_ctx
+{
+    SphParams p{};
+    cudaStream_t stream = nullptr;
+    std::vector<SphBox> boxes;
+    HostSpecies sp[SPH_NUM_SPECIES];
+    bool allocated = false;     //!< device buffers exist for (allocN, allocCells, allocBoxes)
+    bool deviceCurrent = false; //!< the device state holds the latest species data
+    bool mirrorStale = false;   //!< the host mirror is older than the device state
+    bool densityValid = false;
+    bool forceValid = false;
+    uint32_t n = 0, ncells = 0;
+    uint32_t allocN = 0, allocCells = 0, allocBoxes = 0;
+    std::vector<sph::BoxDev> boxDesc;
+    sph::DevCtx dc{};
+    sph::PhysArgs pa{};
+    std::vector<void*> allocs;
+    double* boxOut = nullptr;
+    std::vector<double*> staging;
+    bool useGraph = false;
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    int parity = 0;
+    std::vector<cudaEvent_t> events;
+    double timings[5] = {0, 0, 0, 0, 0};
+
+    ~sph_ctx()
+    {
+        release();
+        for(cudaEvent_t e : events)
+            cudaEventDestroy(e);
+        if(stream)
+            cudaStreamDestroy(stream);
+    }
+
+    void dropGraphs()
+    {
+        for(auto& g : graphs)
+            if(g)
+            {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+
+    void release()
+    {
+        dropGraphs();
+        if(stream)
+            cudaStreamSynchronize(stream);
+        for(void* a : allocs)
+            cudaFree(a);
+        allocs.clear();
+        staging.clear();
+        dc = sph::DevCtx{};
+        boxOut = nullptr;
+        allocated = false;
+        deviceCurrent = false;
+        densityValid = false;
+        forceValid = false;
+        parity = 0;
+    }
+
+    template<typename T>
+    int alloc(T*& out, size_t count)
+    {
+        out = nullptr;
+        if(count == 0)
+            count = 1;
+        void* ptr = nullptr;
+        cudaError_t const e = cudaMalloc(&ptr, count * sizeof(T));
+        if(e != cudaSuccess)
+            return fail(
+                SPH_ERR_NOMEM,
+                std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " + cudaGetErrorString(e));
+        allocs.push_back(ptr);
+        out = static_cast<T*>(ptr);
+        return SPH_OK;
+    }
+
+    int allocMaster(sph::Master& m)
+    {
+        int st = SPH_OK;
+        for(int a = 0; a < 3 && !st; ++a)
+            st = alloc(m.x[a], n);
+        for(int a = 0; a < 3 && !st; ++a)
+            st = alloc(m.v[a], n);
+        for(int a = 0; a < 3 && !st; ++a)
+            st = alloc(m.B[a], n);
+        if(!st)
+            st = alloc(m.u, n);
+        if(!st)
+            st = alloc(m.m, n);
+        if(!st)
+            st = alloc(m.h, n);
+        if(!st)
+            st = alloc(m.rho, n);
+        if(!st)
+            st = alloc(m.psi, n);
+        if(!st)
+            st = alloc(m.id, n);
+        if(!st)
+            st = alloc(m.box, n);
+        if(!st)
+            st = alloc(m.role, n);
+        return st;
+    }
+
+    static double* masterCol(sph::Master const& m, int c)
+    {
+        switch(c)
+        {
+        case cX:
+        case cY:
+        case cZ:
+            return m.x[c - cX];
+        case cVX:
+        case cVY:
+        case cVZ:
+            return m.v[c - cVX];
+        case cU:
+            return m.u;
+        case cM:
+            return m.m;
+        case cH:
+            return m.h;
+        case cRho:
+            return m.rho;
+        case cBX:
+        case cBY:
+        case cBZ:
+            return m.B[c - cBX];
+        case cPsi:
+            return m.psi;
+        }
+        return nullptr;
+    }
+
+    double colDefault(int c) const
+    {
+        return c == cH ? p.h0 : 0.0;
+    }
+
+    void physArgs()
+    {
+        pa.gamma = p.gamma;
+        pa.alpha = p.alpha;
+        pa.beta = p.beta;
+        pa.avEps = p.av_eps;
+        pa.mu0 = p.mu0 > 0 ? p.mu0 : 1.0;
+        pa.cfl = p.cfl;
+        pa.cflForce = p.cfl_force;
+        pa.sigma = p.dedner_sigma;
+        pa.h0 = p.h0;
+        pa.physics = p.physics;
+        pa.cull = p.cull;
+    }
+
+    int stagingCols(size_t k)
+    {
+        while(staging.size() < k)
+        {
+            double* s = nullptr;
+            int st = alloc(s, n);
+            if(st)
+                return st;
+            staging.push_back(s);
+        }
+        return SPH_OK;
+    }
+
+    int layout();
+    int allocate();
+    int uploadMirror();
+    int downloadMirror();
+    int ensureDevice();
+    int probeListCapacity();
+    int growLists(uint32_t need);
+    int build(bool drift);
+    int checkStatus(char const* where);
+    int densityPass();
+    int forcePass();
+    int stepOnce(cudaEvent_t const* ev);
+    int steps(int32_t nsteps, double dt);
+    int setSpeciesFast(int32_t id, SphSoAView const* v);
+};
+
+//! Species offsets, host-side validation and the cell grid of every box.
+int sph_ctx::layout()
+{
+    uint64_t total = 0;
+    for(auto& s : sp)
+        if(s.set)
+        {
+            s.offset = uint32_t(total);
+            total += uint64_t(s.n);
+        }
+    if(total == 0)
+        return fail(SPH_ERR_STATE, "no particles: call sph_set_species first");
+    if(total >= sph::kMaxParticles)
+        return fail(SPH_ERR_UNSUPPORTED, "more than 2^27 particles in one context");
+    n = uint32_t(total);
+    int const sup = supportOf(p.kernel);
+    if(boxes.empty())
+    {
+        // Default domain: the particles' bounding box plus one radius, open.
+        SphBox b{};
+        double hmax = p.h0;
+        for(int a = 0; a < 3; ++a)
+        {
+            b.lo[a] = 1e300;
+            b.hi[a] = -1e300;
+        }
+        for(auto& s : sp)
+            for(int64_t i = 0; s.set && i < s.n; ++i)
+            {
+                for(int a = 0; a < 3; ++a)
+                {
+                    b.lo[a] = std::min(b.lo[a], s.col[cX + a][i]);
+                    b.hi[a] = std::max(b.hi[a], s.col[cX + a][i]);
+                }
+                hmax = std::max(hmax, s.col[cH][i]);
+            }
+        double const m = cellRadius(sup, hmax);
+        for(int a = 0; a < 3; ++a)
+        {
+            b.lo[a] -= m;
+            b.hi[a] += m;
+        }
+        boxes.push_back(b);
+    }
+    int32_t const nbox = int32_t(boxes.size());
+    std::vector<double> hmax(nbox, p.cull == SPH_CULL_PAIR_MAX ? 0.0 : p.h0);
+    for(auto& s : sp)
+    {
+        if(!s.set)
+            continue;
+        for(int64_t i = 0; i < s.n; ++i)
+        {
+            int32_t const b = s.box[i];
+            if(b < 0 || b >= nbox)
+                return fail(SPH_ERR_INVALID, "box_id out of range");
+            SphBox const& B = boxes[b];
+            for(int a = 0; a < 3; ++a)
+            {
+                double const x = s.col[cX + a][i];
+                if(!std::isfinite(x))
+                    return fail(SPH_ERR_NONFINITE, "non-finite position in the input");
+                if(!B.periodic[a] && (x < B.lo[a] || x > B.hi[a]))
+                    return fail(SPH_ERR_OUTSIDE, "particle outside a non-periodic box axis");
+            }
+            if(!(s.col[cH][i] > 0.0) || !std::isfinite(s.col[cH][i]))
+                return fail(SPH_ERR_NONFINITE, "smoothing length must be positive and finite");
+            if((s.roles & SPH_ROLE_SOURCE) && !(s.col[cM][i] > 0.0))
+                return fail(SPH_ERR_NONFINITE, "source particle mass must be positive");
+            if(p.cull == SPH_CULL_PAIR_MAX)
+                hmax[b] = std::max(hmax[b], s.col[cH][i]);
+        }
+    }
+    boxDesc.assign(nbox, sph::BoxDev{});
+    uint64_t cellBase = 0;
+    for(int32_t b = 0; b < nbox; ++b)
+    {
+        SphBox const& B = boxes[b];
+        double const rc = cellRadius(sup, hmax[b]);
+        sph::BoxDev& d = boxDesc[b];
+        uint64_t cells = 1;
+        for(int a = 0; a < 3; ++a)
+        {
+            d.lo[a] = B.lo[a];
+            d.L[a] = B.hi[a] - B.lo[a];
+            if(!(d.L[a] > 0.0))
+                return fail(SPH_ERR_INVALID, "box with non-positive extent");
+            d.periodic[a] = B.periodic[a] ? 1 : 0;
+            double const nd = std::floor(d.L[a] / rc);
+            d.n[a] = nd < 1.0 ? 1 : (nd > 1.0e6 ? 1000000 : int32_t(nd));
+            d.edge[a] = d.L[a] / d.n[a];
+            d.edgef[a] = float(d.edge[a]);
+            if(d.periodic[a] && d.L[a] < rc)
+                return fail(SPH_ERR_UNSUPPORTED, "periodic box thinner than the interaction radius");
+            cells *= uint64_t(d.n[a]);
+        }
+        d.cellBase = uint32_t(cellBase);
+        d.ncells = uint32_t(cells);
+        cellBase += cells;
+        if(cellBase * 2 + 1 >= (1ull << 32))
+            return fail(SPH_ERR_UNSUPPORTED, "too many cells (2^31)");
+    }
+    ncells = uint32_t(cellBase);
+    return SPH_OK;
+}
+
+int sph_ctx::allocate()
+{
+    release();
+    physArgs();
+    uint32_t const nbox = uint32_t(boxDesc.size());
+    dc.n = n;
+    dc.nbox = nbox;
+    int st = SPH_OK;
+    if((st = alloc(dc.boxes, nbox)) || (st = allocMaster(dc.cur)) || (st = allocMaster(dc.alt)))
+        return st;
+    for(int a = 0; a < 3 && !st; ++a)
+        st = alloc(dc.d.dvdt[a], n);
+    for(int a = 0; a < 3 && !st; ++a)
+        st = alloc(dc.d.dBdt[a], n);
+    if(st || (st = alloc(dc.d.dudt, n)) || (st = alloc(dc.d.dpsidt, n)) || (st = alloc(dc.d.divB, n)))
+        return st;
+    if(p.precision == SPH_PREC_FP64)
+    {
+        if((st = alloc(dc.r64.pm, n)) || (st = alloc(dc.r64.hc, n)) || (st = alloc(dc.r64.fv, n))
+           || (st = alloc(dc.r64.ft, n)) || (st = alloc(dc.r64.fb, n)))
+            return st;
+    }
+    else
+    {
+        if((st = alloc(dc.r32.pm, n)) || (st = alloc(dc.r32.hc, n)) || (st = alloc(dc.r32.fv, n))
+           || (st = alloc(dc.r32.ft, n)) || (st = alloc(dc.r32.fb, n)))
+            return st;
+    }
+    dc.cells.ncells = ncells;
+    if((st = alloc(dc.cells.start, ncells)) || (st = alloc(dc.cells.mid, ncells)) || (st = alloc(dc.cells.end, ncells)))
+        return st;
+    if((st = alloc(dc.keysA, n)) || (st = alloc(dc.valsA, n)) || (st = alloc(dc.keysB, n)) || (st = alloc(dc.valsB, n))
+       || (st = alloc(dc.sortScratch, sph::radixScratchWords(n))))
+        return st;
+    if((st = alloc(dc.status, sph::kStatWords)) || (st = alloc(dc.scal, 1)) || (st = alloc(dc.diag, sph::kDiagWords)))
+        return st;
+    dc.nPartialBlocks = sph::partialBlocks(n);
+    if((st = alloc(dc.partials, size_t(dc.nPartialBlocks) * sph::kDiagWords))
+       || (st = alloc(boxOut, size_t(nbox) * sph::kDiagWords)) || (st = alloc(dc.lists.count, n)))
+        return st;
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.diag, 0, sizeof(double) * sph::kDiagWords, stream));
+    dc.keyBits = 1;
+    while((uint64_t(1) << dc.keyBits) <= uint64_t(ncells) * 2)
+        ++dc.keyBits;
+    dc.lists.cap = 0;
+    dc.lists.list = nullptr;
+    sph::configurePairKernels();
+    allocN = n;
+    allocCells = ncells;
+    allocBoxes = nbox;
+    allocated = true;
+    return SPH_OK;
+}
+
+//! Host mirror -> device state in input order (id[p] = p).
+int sph_ctx::uploadMirror()
+{
+    std::vector<double> buf(n);
+    for(int c = 0; c < kHostCols; ++c)
+    {
+        for(auto& s : sp)
+            if(s.set)
+                std::copy(s.col[c].begin(), s.col[c].end(), buf.begin() + s.offset);
+        SPH_CUDA_TRY(cudaMemcpyAsync(masterCol(dc.cur, c), buf.data(), size_t(n) * 8, cudaMemcpyHostToDevice, stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    }
+    std::vector<uint32_t> ids(n);
+    std::vector<int32_t> bx(n);
+    std::vector<uint8_t> roles(n);
+    for(auto& s : sp)
+        if(s.set)
+            for(int64_t i = 0; i < s.n; ++i)
+            {
+                ids[s.offset + i] = uint32_t(s.offset + i);
+                bx[s.offset + i] = s.box[i];
+                roles[s.offset + i] = uint8_t(s.roles);
+            }
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.cur.id, ids.data(), size_t(n) * 4, cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.cur.box, bx.data(), size_t(n) * 4, cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.cur.role, roles.data(), size_t(n), cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(
+        dc.boxes,
+        boxDesc.data(),
+        sizeof(sph::BoxDev) * boxDesc.size(),
+        cudaMemcpyHostToDevice,
+        stream));
+    sph::StepScalars sc{};
+    sc.dt = p.dt;
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.scal, &sc, sizeof(sc), cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    mirrorStale = false;
+    deviceCurrent = true;
+    densityValid = false;
+    forceValid = false;
+    return SPH_OK;
+}
+
+//! Device state -> host mirror (input order), before a re-layout.
+int sph_ctx::downloadMirror()
+{
+    int st = stagingCols(1);
+    if(st)
+        return st;
+    for(auto& s : sp)
+    {
+        if(!s.set)
+            continue;
+        for(int c = 0; c < kHostCols; ++c)
+        {
+            sph::launchUnpermute(n, dc.cur.id, masterCol(dc.cur, c), staging[0], stream);
+            SPH_CUDA_TRY(cudaMemcpyAsync(
+                s.col[c].data(),
+                staging[0] + s.offset,
+                size_t(s.n) * 8,
+                cudaMemcpyDeviceToHost,
+                stream));
+            SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+        }
+    }
+    mirrorStale = false;
+    return SPH_OK;
+}
+
+int sph_ctx::probeListCapacity()
+{
+    uint32_t capN = uint32_t(p.max_neighbours);
+    if(capN == 0)
+    {
+        int st = build(false);
+        if(st)
+            return st;
+        sph::launchDensity(dc, pa, p.kernel, p.precision, true, stream);
+        uint32_t stat[sph::kStatWords];
+        SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost, stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+        capN = uint32_t(double(stat[sph::kStatMaxCount]) * 1.25) + 16;
+    }
+    return growLists(capN);
+}
+
+//! (Re)allocates the neighbour lists with room for `need` entries per target.
+int sph_ctx::growLists(uint32_t need)
+{
+    uint32_t const capN = std::max<uint32_t>(32, (need + 7) & ~7u);
+    SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    if(dc.lists.list)
+    {
+        auto it = std::find(allocs.begin(), allocs.end(), static_cast<void*>(dc.lists.list));
+        if(it != allocs.end())
+        {
+            cudaFree(*it);
+            allocs.erase(it);
+        }
+        dc.lists.list = nullptr;
+    }
+    uint32_t* list = nullptr;
+    int st = alloc(list, size_t(n) * capN);
+    if(st)
+        return st;
+    dc.lists.list = list;
+    dc.lists.cap = capN;
+    dropGraphs();
+    densityValid = false;
+    forceValid = false;
+    return SPH_OK;
+}
+
+int sph_ctx::ensureDevice()
+{
+    if(deviceCurrent)
+        return SPH_OK;
+    if(allocated && mirrorStale)
+    {
+        int st = downloadMirror();
+        if(st)
+            return st;
+    }
+    int st = layout();
+    if(st)
+        return st;
+    bool const fresh = !allocated || n != allocN || ncells != allocCells || boxDesc.size() != allocBoxes;
+    if(fresh && (st = allocate()))
+        return st;
+    physArgs();
+    if((st = uploadMirror()))
+        return st;
+    if(fresh && (st = probeListCapacity()))
+        return st;
+    return SPH_OK;
+}
+
+//! Drift (optional) + cell keys + sort + cell ranges + permute/pack.
+int sph_ctx::build(bool drift)
+{
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.status, 0, sizeof(uint32_t) * sph::kStatWords, stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->chBits, 0, sizeof(unsigned long long), stream));
+    sph::launchDriftKeys(dc, drift, stream);
+    bool const inB = sph::radixSortPairs(dc.keysA, dc.valsA, dc.keysB, dc.valsB, n, dc.keyBits, dc.sortScratch, stream);
+    uint32_t const* keys = inB ? dc.keysB : dc.keysA;
+    uint32_t const* perm = inB ? dc.valsB : dc.valsA;
+    sph::launchCellRanges(dc, keys, stream);
+    sph::launchPermute(dc, perm, pa, p.precision, stream);
+    std::swap(dc.cur, dc.alt);
+    parity ^= 1;
+    return SPH_OK;
+}
+
+int sph_ctx::densityPass()
+{
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.lists.count, 0xff, size_t(n) * 4, stream));
+    sph::launchDensity(dc, pa, p.kernel, p.precision, false, stream);
+    return SPH_OK;
+}
+
+int sph_ctx::forcePass()
+{
+    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->dtBits, 0x7f, sizeof(unsigned long long), stream));
+    sph::launchForce(dc, pa, p.kernel, p.precision, stream);
+    return SPH_OK;
+}
+
+int sph_ctx::checkStatus(char const* where)
+{
+    uint32_t stat[sph::kStatWords];
+    SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost, stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    SPH_CUDA_TRY(cudaGetLastError());
+    if(stat[sph::kStatNonFinite])
+        return fail(
+            SPH_ERR_NONFINITE,
+            std::string(where) + ": " + std::to_string(stat[sph::kStatNonFinite]) + " particles with non-finite positions");
+    if(stat[sph::kStatOutside])
+        return fail(
+            SPH_ERR_OUTSIDE,
+            std::string(where) + ": " + std::to_string(stat[sph::kStatOutside]) + " particles left a non-periodic box");
+    if(stat[sph::kStatOverflow])
+        return fail(
+            SPH_ERR_OVERFLOW,
+            std::string(where) + ": a neighbour list needed " + std::to_string(stat[sph::kStatOverflow])
+                + " entries, capacity " + std::to_string(dc.lists.cap));
+    return SPH_OK;
+}
+
+//! One runOneStep; ev (5 events or null) brackets build / density / force / kick.
+int sph_ctx::stepOnce(cudaEvent_t const* ev)
+{
+    int st;
+    if(ev)
+        SPH_CUDA_TRY(cudaEventRecord(ev[0], stream));
+    if((st = build(true)))
+        return st;
+    if(ev)
+        SPH_CUDA_TRY(cudaEventRecord(ev[1], stream));
+    if((st = densityPass()))
+        return st;
+    if(ev)
+        SPH_CUDA_TRY(cudaEventRecord(ev[2], stream));
+    if((st = forcePass()))
+        return st;
+    if(ev)
+        SPH_CUDA_TRY(cudaEventRecord(ev[3], stream));
+    sph::launchKick(dc, pa, stream);
+    sph::launchFinalize(dc, (p.physics & SPH_PHYS_CFL) != 0, stream);
+    if(ev)
+        SPH_CUDA_TRY(cudaEventRecord(ev[4], stream));
+    return SPH_OK;
+}
+
+int sph_ctx::steps(int32_t nsteps, double dt)
+{
+    int st = ensureDevice();
+    if(st)
+        return st;
+    if(dt > 0.0)
+        SPH_CUDA_TRY(cudaMemcpyAsync(&dc.scal->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, stream));
+    for(double& t : timings)
+        t = 0.0;
+    bool const graph = useGraph && nsteps >= 2;
+    size_t const nev = size_t(nsteps) * 5 + 2;
+    while(events.size() < nev)
+    {
+        cudaEvent_t e;
+        SPH_CUDA_TRY(cudaEventCreate(&e));
+        events.push_back(e);
+    }
+    cudaEvent_t const eBeg = events[0], eEnd = events[1];
+    SPH_CUDA_TRY(cudaEventRecord(eBeg, stream));
+    int32_t done = 0;
+    if(graph)
+    {
+        while(nsteps - done >= 2)
+        {
+            cudaGraphExec_t& g = graphs[parity];
+            if(!g)
+            {
+                cudaGraph_t raw = nullptr;
+                SPH_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                int const s1 = stepOnce(nullptr);
+                int const s2 = s1 ? s1 : stepOnce(nullptr);
+                cudaError_t const ce = cudaStreamEndCapture(stream, &raw);
+                if(s2)
+                    return s2;
+                SPH_CUDA_TRY(ce);
+                cudaError_t const ie = cudaGraphInstantiate(&g, raw, 0);
+                cudaGraphDestroy(raw);
+                SPH_CUDA_TRY(ie);
+            }
+            SPH_CUDA_TRY(cudaGraphLaunch(g, stream));
+            done += 2;
+        }
+    }
+    int32_t const eager0 = done;
+    for(; done < nsteps; ++done)
+        if((st = stepOnce(graph ? nullptr : &events[2 + size_t(done) * 5])))
+            return st;
+    SPH_CUDA_TRY(cudaEventRecord(eEnd, stream));
+    st = checkStatus("sph_step");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, eBeg, eEnd);
+    timings[4] = ms;
+    if(!graph)
+        for(int32_t s = eager0; s < nsteps; ++s)
+            for(int k = 0; k < 4; ++k)
+            {
+                cudaEventElapsedTime(&ms, events[2 + size_t(s) * 5 + k], events[2 + size_t(s) * 5 + k + 1]);
+                timings[k] += ms;
+            }
+    densityValid = true;
+    forceValid = true;
+    if(st == SPH_ERR_OVERFLOW)
+    {
+        // The lists grow for the next call; this call's result is not valid.
+        uint32_t stat[sph::kStatWords];
+        SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
+        int const g = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16);
+        if(g)
+            return g;
+    }
+    return st;
+}
+
+//! Species of unchanged size on an allocated context: caller columns -> staging
+//! (input order) -> gather into the sorted state by particle id.
+int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
+{
+    HostSpecies& s = sp[id];
+    int st = stagingCols(kHostCols);
+    if(st)
+        return st;
+    for(int c = 0; c < kHostCols; ++c)
+    {
+        double const* src = viewCol(v, c);
+        if(c == cH && src)
+            for(int64_t i = 0; i < s.n; ++i)
+                if(!(src[i] > 0.0) || !std::isfinite(src[i]))
+                    return fail(SPH_ERR_NONFINITE, "smoothing length must be positive and finite");
+        if(c == cM && src && (s.roles & SPH_ROLE_SOURCE))
+            for(int64_t i = 0; i < s.n; ++i)
+                if(!(src[i] > 0.0))
+                    return fail(SPH_ERR_NONFINITE, "source particle mass must be positive");
+    }
+    for(int c = 0; c < kHostCols; ++c)
+    {
+        double const* src = viewCol(v, c);
+        double* stage = staging[c];
+        if(src)
+            SPH_CUDA_TRY(cudaMemcpyAsync(stage + s.offset, src, size_t(s.n) * 8, cudaMemcpyHostToDevice, stream));
+        sph::launchGatherSpecies(
+            n,
+            dc.cur.id,
+            s.offset,
+            uint32_t(s.n),
+            src ? stage : nullptr,
+            colDefault(c),
+            masterCol(dc.cur, c),
+            stream);
+    }
+    if(v && v->box_id)
+    {
+        for(int64_t i = 0; i < s.n; ++i)
+            if(v->box_id[i] < 0 || uint32_t(v->box_id[i]) >= allocBoxes)
+                return fail(SPH_ERR_INVALID, "box_id out of range");
+        int32_t* stage = reinterpret_cast<int32_t*>(staging[0]);
+        SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(stage + s.offset, v->box_id, size_t(s.n) * 4, cudaMemcpyHostToDevice, stream));
+        sph::launchGatherSpeciesInt(n, dc.cur.id, s.offset, uint32_t(s.n), stage, dc.cur.box, stream);
+    }
+    SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    mirrorStale = true;
+    densityValid = false;
+    forceValid = false;
+    return SPH_OK;
+}
+
+// ============================================================== C ABI
+extern "C" {
+
+int sph_default_params(SphParams* p)
+{
+    if(!p)
+        return fail(SPH_ERR_INVALID, "null params");
+    *p = SphParams{};
+    p->kernel = SPH_KERNEL_CUBIC;
+    p->precision = SPH_PREC_FP32_COMP;
+    p->cull = SPH_CULL_GLOBAL;
+    p->physics = 0;
+    p->gamma = 5.0 / 3.0;
+    p->h0 = 0.05;
+    p->dt = 0.01;
+    p->alpha = 1.0;
+    p->beta = 2.0;
+    p->av_eps = 0.01;
+    p->cfl = 0.3;
+    p->cfl_force = 0.25;
+    p->dedner_sigma = 1.0;
+    p->mu0 = 1.0;
+    p->max_neighbours = 0;
+    p->device = 0;
+    return SPH_OK;
+}
+
+int sph_create(SphParams const* params, sph_ctx** out)
+{
+    if(!params || !out)
+        return fail(SPH_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int st = validateParams(*params);
+    if(st)
+        return st;
+    SPH_CUDA_TRY(cudaSetDevice(params->device));
+    sph_ctx* c = new(std::nothrow) sph_ctx();
+    if(!c)
+        return fail(SPH_ERR_NOMEM, "host allocation failed");
+    c->p = *params;
+    cudaError_t const e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if(e != cudaSuccess)
+    {
+        delete c;
+        return fail(SPH_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return SPH_OK;
+}
+
+int sph_destroy(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    cudaSetDevice(ctx->p.device);
+    delete ctx;
+    return SPH_OK;
+}
+
+int sph_set_boxes(sph_ctx* ctx, int32_t nbox, SphBox const* boxes)
+{
+    if(!ctx || nbox < 1 || !boxes)
+        return fail(SPH_ERR_INVALID, "sph_set_boxes: bad arguments");
+    for(int32_t b = 0; b < nbox; ++b)
+        for(int a = 0; a < 3; ++a)
+            if(!(boxes[b].hi[a] > boxes[b].lo[a]) || !std::isfinite(boxes[b].lo[a]) || !std::isfinite(boxes[b].hi[a]))
+                return fail(SPH_ERR_INVALID, "sph_set_boxes: empty or non-finite box");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    if(ctx->allocated && ctx->mirrorStale)
+    {
+        int st = ctx->downloadMirror();
+        if(st)
+            return st;
+    }
+    ctx->boxes.assign(boxes, boxes + nbox);
+    ctx->deviceCurrent = false;
+    return SPH_OK;
+}
+
+int sph_set_species(sph_ctx* ctx, int32_t species_id, uint32_t roles, int64_t n, SphSoAView const* v)
+{
+    if(!ctx || species_id < 0 || species_id >= SPH_NUM_SPECIES || n < 0 || (n > 0 && !v))
+        return fail(SPH_ERR_INVALID, "sph_set_species: bad arguments");
+    if(n > 0 && (!v->pos[0] || !v->pos[1] || !v->pos[2]))
+        return fail(SPH_ERR_INVALID, "sph_set_species: positions are required");
+    if((roles & SPH_ROLE_SOURCE) && n > 0 && !v->mass)
+        return fail(SPH_ERR_INVALID, "sph_set_species: source species need masses");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    HostSpecies& s = ctx->sp[species_id];
+    if(ctx->allocated && ctx->deviceCurrent && s.set && s.n == n && s.roles == roles)
+        return ctx->setSpeciesFast(species_id, v);
+    if(ctx->allocated && ctx->mirrorStale)
+    {
+        int st = ctx->downloadMirror();
+        if(st)
+            return st;
+    }
+    s.set = n > 0;
+    s.roles = roles;
+    s.n = n;
+    for(int c = 0; c < kHostCols; ++c)
+    {
+        double const* src = viewCol(v, c);
+        s.col[c].assign(size_t(n), ctx->colDefault(c));
+        if(src)
+            std::copy(src, src + n, s.col[c].begin());
+    }
+    s.box.assign(size_t(n), 0);
+    if(v && v->box_id)
+        std::copy(v->box_id, v->box_id + n, s.box.begin());
+    ctx->deviceCurrent = false;
+    return SPH_OK;
+}
+
+int sph_density(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->ensureDevice();
+    if(st || (st = ctx->build(false)) || (st = ctx->densityPass()))
+        return st;
+    st = ctx->checkStatus("sph_density");
+    if(st == SPH_ERR_OVERFLOW)
+    {
+        uint32_t stat[sph::kStatWords];
+        SPH_CUDA_TRY(cudaMemcpy(stat, ctx->dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
+        if((st = ctx->growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16)))
+            return st;
+        SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.status, 0, sizeof(uint32_t) * sph::kStatWords, ctx->stream));
+        SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->pairs, 0, sizeof(unsigned long long), ctx->stream));
+        SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->chBits, 0, sizeof(unsigned long long), ctx->stream));
+        if((st = ctx->densityPass()) || (st = ctx->checkStatus("sph_density")))
+            return st;
+    }
+    else if(st)
+        return st;
+    ctx->densityValid = true;
+    ctx->forceValid = false;
+    return SPH_OK;
+}
+
+int sph_hydro(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    if(!ctx->densityValid)
+        return fail(SPH_ERR_STATE, "sph_hydro needs the density of the current state (call sph_density first)");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->forcePass();
+    if(st || (st = ctx->checkStatus("sph_hydro")))
+        return st;
+    ctx->forceValid = true;
+    return SPH_OK;
+}
+
+int sph_mhd(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    if(!(ctx->p.physics & SPH_PHYS_MHD))
+        return fail(SPH_ERR_STATE, "sph_mhd needs SPH_PHYS_MHD in the context's params");
+    return sph_hydro(ctx);
+}
+
+int sph_step(sph_ctx* ctx, int32_t n_steps, double dt)
+{
+    if(!ctx || n_steps < 0 || !std::isfinite(dt))
+        return fail(SPH_ERR_INVALID, "sph_step: bad arguments");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    return ctx->steps(n_steps, dt);
+}
+
+int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* v)
+{
+    if(!ctx || !v || species_id < 0 || species_id >= SPH_NUM_SPECIES)
+        return fail(SPH_ERR_INVALID, "sph_get_species: bad arguments");
+    HostSpecies const& s = ctx->sp[species_id];
+    if(!s.set)
+        return fail(SPH_ERR_STATE, "sph_get_species: species not set");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->ensureDevice();
+    if(st)
+        return st;
+    sph::DevCtx& d = ctx->dc;
+    // (device column, host destination) pairs; every column is unpermuted into
+    // its own staging column, then all copies run back to back.
+    std::vector<std::pair<double const*, double*>> cols;
+    for(int a = 0; a < 3; ++a)
+    {
+        cols.push_back({d.cur.x[a], v->pos[a]});
+        cols.push_back({d.cur.v[a], v->vel[a]});
+        cols.push_back({d.cur.B[a], v->B[a]});
+    }
+    cols.push_back({d.cur.m, v->mass});
+    cols.push_back({d.cur.h, v->h});
+    cols.push_back({d.cur.rho, v->density});
+    cols.push_back({d.cur.u, v->u});
+    cols.push_back({d.cur.psi, v->psi});
+    if(ctx->forceValid)
+    {
+        for(int a = 0; a < 3; ++a)
+            cols.push_back({d.d.dvdt[a], v->dvdt[a]});
+        cols.push_back({d.d.dudt, v->dudt});
+        if(ctx->p.physics & SPH_PHYS_MHD)
+        {
+            for(int a = 0; a < 3; ++a)
+                cols.push_back({d.d.dBdt[a], v->dBdt[a]});
+            cols.push_back({d.d.dpsidt, v->dpsidt});
+            cols.push_back({d.d.divB, v->divB});
+        }
+    }
+    size_t k = 0;
+    for(auto const& c : cols)
+        k += c.second ? 1 : 0;
+    if((st = ctx->stagingCols(k + 1)))
+        return st;
+    k = 0;
+    for(auto const& c : cols)
+    {
+        if(!c.second)
+            continue;
+        double* stage = ctx->staging[k++];
+        sph::launchUnpermute(ctx->n, d.cur.id, c.first, stage, ctx->stream);
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.second, stage + s.offset, size_t(s.n) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if(v->box_id)
+    {
+        int32_t* istage = reinterpret_cast<int32_t*>(ctx->staging[k]);
+        sph::launchUnpermuteInt(ctx->n, d.cur.id, reinterpret_cast<uint32_t const*>(d.cur.box), istage, ctx->stream);
+        SPH_CUDA_TRY(cudaMemcpyAsync(v->box_id, istage + s.offset, size_t(s.n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts)
+{
+    if(!ctx || !counts || species_id < 0 || species_id >= SPH_NUM_SPECIES)
+        return fail(SPH_ERR_INVALID, "sph_get_neighbour_counts: bad arguments");
+    HostSpecies const& s = ctx->sp[species_id];
+    if(!s.set)
+        return fail(SPH_ERR_STATE, "species not set");
+    if(!ctx->densityValid)
+        return fail(SPH_ERR_STATE, "no neighbour build yet (call sph_density or sph_step)");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->stagingCols(1);
+    if(st)
+        return st;
+    int32_t* istage = reinterpret_cast<int32_t*>(ctx->staging[0]);
+    sph::launchUnpermuteInt(ctx->n, ctx->dc.cur.id, ctx->dc.lists.count, istage, ctx->stream);
+    SPH_CUDA_TRY(cudaMemcpyAsync(counts, istage + s.offset, size_t(s.n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+namespace
+{
+    int reduceBoxes(sph_ctx* ctx, std::vector<double>& perBox, sph::StepScalars& sc, double* diag)
+    {
+        int st = ctx->ensureDevice();
+        if(st)
+            return st;
+        sph::launchBoxReduce(ctx->dc, ctx->pa, ctx->boxOut, ctx->stream);
+        perBox.resize(size_t(ctx->dc.nbox) * sph::kDiagWords);
+        SPH_CUDA_TRY(cudaMemcpyAsync(perBox.data(), ctx->boxOut, perBox.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(&sc, ctx->dc.scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(diag, ctx->dc.diag, sizeof(double) * sph::kDiagWords, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return SPH_OK;
+    }
+
+    void fillDiag(SphDiag& o, double const* a, sph::StepScalars const& sc, double const* diag)
+    {
+        o.e_kin = a[0];
+        o.e_int = a[1];
+        o.e_mag = a[2];
+        o.mom[0] = a[3];
+        o.mom[1] = a[4];
+        o.mom[2] = a[5];
+        o.divb_mean = a[7] > 0 ? a[6] / a[7] : 0.0;
+        o.divb_max = a[8];
+        o.n_targets = int64_t(a[9]);
+        o.time = sc.time;
+        o.dt = diag[10];
+        o.dt_next = sc.dt;
+        o.c_h = __builtin_bit_cast(double, sc.chBits);
+        o.pairs = double(sc.pairs);
+        o.steps = sc.steps;
+        o.pairs_total = sc.pairsAccum;
+    }
+} // namespace
+
+int sph_reduce(sph_ctx* ctx, SphDiag* out)
+{
+    if(!ctx || !out)
+        return fail(SPH_ERR_INVALID, "sph_reduce: bad arguments");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    std::vector<double> pb;
+    sph::StepScalars sc{};
+    double diag[sph::kDiagWords] = {};
+    int st = reduceBoxes(ctx, pb, sc, diag);
+    if(st)
+        return st;
+    double a[sph::kDiagWords] = {};
+    for(uint32_t b = 0; b < ctx->dc.nbox; ++b)
+        for(int k = 0; k < sph::kDiagWords; ++k)
+        {
+            double const v = pb[size_t(b) * sph::kDiagWords + k];
+            a[k] = (k == 8) ? std::max(a[k], v) : a[k] + v;
+        }
+    *out = SphDiag{};
+    fillDiag(*out, a, sc, diag);
+    return SPH_OK;
+}
+
+int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
+{
+    if(!ctx || !out || nbox < 1)
+        return fail(SPH_ERR_INVALID, "sph_ensemble_reduce: bad arguments");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    std::vector<double> pb;
+    sph::StepScalars sc{};
+    double diag[sph::kDiagWords] = {};
+    int st = reduceBoxes(ctx, pb, sc, diag);
+    if(st)
+        return st;
+    if(uint32_t(nbox) != ctx->dc.nbox)
+        return fail(SPH_ERR_INVALID, "sph_ensemble_reduce: nbox differs from the context's box count");
+    for(int32_t b = 0; b < nbox; ++b)
+    {
+        out[b] = SphDiag{};
+        fillDiag(out[b], &pb[size_t(b) * sph::kDiagWords], sc, diag);
+    }
+    return SPH_OK;
+}
+
+int sph_get_timings(sph_ctx* ctx, int32_t n, double* ms)
+{
+    if(!ctx || !ms || n < 0)
+        return fail(SPH_ERR_INVALID, "sph_get_timings: bad arguments");
+    for(int32_t i = 0; i < n && i < 5; ++i)
+        ms[i] = ctx->timings[i];
+    return SPH_OK;
+}
+
+int sph_use_graph(sph_ctx* ctx, int32_t on)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    ctx->useGraph = on != 0;
+    return SPH_OK;
+}
+
+const char* sph_last_error_string(void)
+{
+    return g_lastError.c_str();
+}
+} // extern "C"

@@ -1,0 +1,668 @@
+// Pair kernels: neighbour build + density summation, and the force pass.
+//
+// Replaces the reference's pair engine (interact() -> FrameInteractionKernel /
+// UnifiedFrameInteractionKernel, spmacc/particles/algorithms/InteractParticles.hpp:140-199,
+// ParticleParticleInteraction.hpp:219-612) and the functors it drives
+// (AccumulateDensity, DensitySummation.hpp:50-74; HydroInteraction,
+// HydroForces.hpp:86-176), plus the viscosity, SPMHD and Dedner terms the
+// reference lacks.
+//
+// Density kernel: one warp per target cell (cell edge >= cull radius).  The
+// warp stages the 27-cell stencil's sources into shared memory with the
+// stencil shift already added (the reference's origin-shifted staging,
+// ParticleParticleInteraction.hpp:241-265), each lane owns one target and
+// sweeps the staged candidates with broadcast reads, culling with r^2
+// evaluated unfused in x, y, z order exactly as the reference's CPU path does.
+// Accepted pairs are written to the target's neighbour-list row (sorted source
+// index + stencil slot); the density sum then runs over the compact row, so
+// the kernel arithmetic runs on accepted pairs only, with every lane busy.
+// The epilogue writes rho (FP64) and the target's derived record for the force
+// pass.
+//
+// Force kernel: one thread per sorted target, over its list row, gathering the
+// neighbours' 64-byte (FP32) or 128-byte (FP64) records through L1.
+//
+// Precision: FP32 kernels accumulate every per-particle sum with CompAcc
+// (blocks of 8 terms folded by TwoSum); FP64 kernels sum plainly.
+#include "sph_launch.hpp"
+
+namespace sph
+{
+    namespace
+    {
+        constexpr int kDensWarps = 4;
+        constexpr int kForceThreads = 128;
+        constexpr int kBlock = 8; //!< terms per compensated block
+
+        template<typename T>
+        struct PairCfg;
+        template<>
+        struct PairCfg<float>
+        {
+            using V4 = float4;
+            static constexpr int cap = 1024;
+        };
+        template<>
+        struct PairCfg<double>
+        {
+            using V4 = D4;
+            static constexpr int cap = 512;
+        };
+
+        template<typename T>
+        __device__ __forceinline__ Records<typename PairCfg<T>::V4, T> records(DevCtx const& c);
+        template<>
+        __device__ __forceinline__ Records<float4, float> records<float>(DevCtx const& c)
+        {
+            return c.r32;
+        }
+        template<>
+        __device__ __forceinline__ Records<D4, double> records<double>(DevCtx const& c)
+        {
+            return c.r64;
+        }
+
+        // Unfused arithmetic: the reference's CPU evaluation of the pair geometry.
+        __device__ __forceinline__ float mulRn(float a, float b)
+        {
+            return __fmul_rn(a, b);
+        }
+        __device__ __forceinline__ float addRn(float a, float b)
+        {
+            return __fadd_rn(a, b);
+        }
+        __device__ __forceinline__ float subRn(float a, float b)
+        {
+            return __fsub_rn(a, b);
+        }
+        __device__ __forceinline__ double mulRn(double a, double b)
+        {
+            return __dmul_rn(a, b);
+        }
+        __device__ __forceinline__ double addRn(double a, double b)
+        {
+            return __dadd_rn(a, b);
+        }
+        __device__ __forceinline__ double subRn(double a, double b)
+        {
+            return __dsub_rn(a, b);
+        }
+        __device__ __forceinline__ float rsqrtT(float x)
+        {
+            return rsqrtf(x);
+        }
+        __device__ __forceinline__ double rsqrtT(double x)
+        {
+            return rsqrt(x);
+        }
+        __device__ __forceinline__ float rcpT(float x)
+        {
+            return __frcp_rn(x);
+        }
+        __device__ __forceinline__ double rcpT(double x)
+        {
+            return 1.0 / x;
+        }
+
+        template<typename T>
+        __device__ __forceinline__ T edgeOf(BoxDev const& B, int a);
+        template<>
+        __device__ __forceinline__ float edgeOf<float>(BoxDev const& B, int a)
+        {
+            return B.edgef[a];
+        }
+        template<>
+        __device__ __forceinline__ double edgeOf<double>(BoxDev const& B, int a)
+        {
+            return B.edge[a];
+        }
+
+        //! Accumulator: FP32 compensated (CompAcc + block partial) or FP64 plain.
+        template<typename T>
+        struct Acc;
+        template<>
+        struct Acc<float>
+        {
+            CompAcc c;
+            float part = 0.f;
+            __device__ __forceinline__ void add(float x)
+            {
+                part += x;
+            }
+            __device__ __forceinline__ void fold()
+            {
+                c.fold(part);
+                part = 0.f;
+            }
+            __device__ __forceinline__ double value() const
+            {
+                return c.value();
+            }
+        };
+        template<>
+        struct Acc<double>
+        {
+            double s = 0.0;
+            __device__ __forceinline__ void add(double x)
+            {
+                s += x;
+            }
+            __device__ __forceinline__ void fold()
+            {
+            }
+            __device__ __forceinline__ double value() const
+            {
+                return s;
+            }
+        };
+
+        __device__ __forceinline__ uint32_t warpMaxU(uint32_t v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+            return v;
+        }
+        __device__ __forceinline__ unsigned long long warpSumU64(unsigned long long v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v += __shfl_xor_sync(0xffffffffu, v, o);
+            return v;
+        }
+        __device__ __forceinline__ double warpMaxD(double v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            return v;
+        }
+        __device__ __forceinline__ double warpMinD(double v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+            return v;
+        }
+
+        template<int K, typename T, bool PAIRMAX>
+        __global__ void __launch_bounds__(kDensWarps * 32) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
+        {
+            using V4 = typename PairCfg<T>::V4;
+            constexpr int CAP = PairCfg<T>::cap;
+            extern __shared__ __align__(32) unsigned char smem[];
+            int const warp = threadIdx.x >> 5;
+            int const lane = threadIdx.x & 31;
+            V4* sPos = reinterpret_cast<V4*>(smem) + warp * CAP;
+            T* sH = reinterpret_cast<T*>(smem + size_t(kDensWarps) * CAP * sizeof(V4)) + warp * CAP;
+            uint32_t* sEnt = reinterpret_cast<uint32_t*>(smem + size_t(kDensWarps) * CAP * (sizeof(V4) + sizeof(T)))
+                             + warp * CAP;
+            Records<V4, T> const rec = records<T>(c);
+            T const supT = T(Kern<K>::support);
+            T const Rg = mulRn(supT, T(pa.h0));
+            T const R2g = mulRn(Rg, Rg);
+            uint32_t const cap = c.lists.cap;
+            uint32_t const nWarps = gridDim.x * kDensWarps;
+            uint32_t maxCount = 0;
+            unsigned long long pairs = 0;
+            double chMax = 0.0;
+
+            for(uint32_t cell = blockIdx.x * kDensWarps + warp; cell < c.cells.ncells; cell += nWarps)
+            {
+                uint32_t const tBeg = c.cells.start[cell];
+                uint32_t const tEnd = c.cells.mid[cell];
+                if(tBeg >= tEnd)
+                    continue;
+                BoxDev const& B = c.boxes[boxOfCell(c.boxes, c.nbox, cell)];
+                uint32_t const lc = cell - B.cellBase;
+                int const cc[3]
+                    = {int(lc % uint32_t(B.n[0])), int((lc / uint32_t(B.n[0])) % uint32_t(B.n[1])),
+                       int(lc / (uint32_t(B.n[0]) * uint32_t(B.n[1])))};
+                // Lane l < 27 describes stencil slot l: its source range and image shift.
+                uint32_t sBeg = 0, sCnt = 0;
+                T sh[3] = {T(0), T(0), T(0)};
+                if(lane < 27)
+                {
+                    bool ok = true;
+                    int nc[3];
+#pragma unroll
+                    for(int a = 0; a < 3; ++a)
+                    {
+                        int const o = stencilOff(lane, a);
+                        nc[a] = cc[a] + o;
+                        if(nc[a] < 0 || nc[a] >= B.n[a])
+                        {
+                            if(B.periodic[a])
+                                nc[a] = (nc[a] + B.n[a]) % B.n[a];
+                            else
+                                ok = false;
+                        }
+                        sh[a] = T(o) * edgeOf<T>(B, a);
+                    }
+                    if(ok)
+                    {
+                        uint32_t const ncell
+                            = B.cellBase + (uint32_t(nc[2]) * uint32_t(B.n[1]) + uint32_t(nc[1])) * uint32_t(B.n[0])
+                              + uint32_t(nc[0]);
+                        sBeg = c.cells.start[ncell];
+                        sCnt = c.cells.end[ncell] - sBeg;
+                    }
+                }
+                uint32_t incl = sCnt;
+#pragma unroll
+                for(int d = 1; d < 32; d <<= 1)
+                {
+                    uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
+                    if(lane >= d)
+                        incl += o;
+                }
+                uint32_t const pre = incl - sCnt;
+                uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+
+                for(uint32_t tc = tBeg; tc < tEnd; tc += 32)
+                {
+                    uint32_t const t = tc + uint32_t(lane);
+                    bool const act = t < tEnd;
+                    V4 own{};
+                    T hi = T(1);
+                    if(act)
+                    {
+                        own = ld4(rec.pm + t);
+                        hi = rec.hc[t];
+                    }
+                    uint32_t const selfEnt = packEntry(t, kCentreSlot);
+                    uint32_t* row = c.lists.list + size_t(t) * cap;
+                    uint32_t nl = 0;
+                    for(uint32_t cb = 0; cb < total; cb += CAP)
+                    {
+                        uint32_t const ce = min(total, cb + uint32_t(CAP));
+                        __syncwarp();
+                        for(int sl = 0; sl < 27; ++sl)
+                        {
+                            uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
+                            uint32_t const n0 = __shfl_sync(0xffffffffu, sCnt, sl);
+                            uint32_t const b0 = __shfl_sync(0xffffffffu, sBeg, sl);
+                            T const sx = __shfl_sync(0xffffffffu, sh[0], sl);
+                            T const sy = __shfl_sync(0xffffffffu, sh[1], sl);
+                            T const sz = __shfl_sync(0xffffffffu, sh[2], sl);
+                            uint32_t const lo = max(p0, cb);
+                            uint32_t const hi2 = min(p0 + n0, ce);
+                            for(uint32_t q = lo + uint32_t(lane); q < hi2; q += 32)
+                            {
+                                uint32_t const j = b0 + (q - p0);
+                                V4 pj = ld4(rec.pm + j);
+                                pj.x = addRn(pj.x, sx);
+                                pj.y = addRn(pj.y, sy);
+                                pj.z = addRn(pj.z, sz);
+                                sPos[q - cb] = pj;
+                                sEnt[q - cb] = packEntry(j, uint32_t(sl));
+                                if constexpr(PAIRMAX)
+                                    sH[q - cb] = rec.hc[j];
+                            }
+                        }
+                        __syncwarp();
+                        if(act)
+                        {
+                            uint32_t const m = ce - cb;
+                            for(uint32_t q = 0; q < m; ++q)
+                            {
+                                V4 const pj = sPos[q];
+                                T const dx = subRn(own.x, pj.x);
+                                T const dy = subRn(own.y, pj.y);
+                                T const dz = subRn(own.z, pj.z);
+                                T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
+                                T R2 = R2g;
+                                if constexpr(PAIRMAX)
+                                {
+                                    T const hj = sH[q];
+                                    T const R = mulRn(supT, hi > hj ? hi : hj);
+                                    R2 = mulRn(R, R);
+                                }
+                                if(r2 < R2)
+                                {
+                                    uint32_t const e = sEnt[q];
+                                    if(e != selfEnt)
+                                    {
+                                        if(!countOnly && nl < cap)
+                                            row[nl] = e;
+                                        ++nl;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    maxCount = max(maxCount, act ? nl : 0u);
+                    pairs += act ? nl : 0u;
+                    if(countOnly || !act)
+                        continue;
+                    // Density over the compact row (DensitySummation.hpp:57-93):
+                    // rho_i = m_i W(0, h_i) + sum_j m_j W(r_ij, h_i).
+                    uint32_t const n = min(nl, cap);
+                    HConst<T> const hk = hconst<K, T>(hi);
+                    Acc<T> rho;
+                    rho.add(own.w * kernelW<K, T>(T(0), hk));
+                    T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
+                    for(uint32_t k0 = 0; k0 < n; k0 += kBlock)
+                    {
+                        uint32_t const k1 = min(n, k0 + kBlock);
+                        for(uint32_t k = k0; k < k1; ++k)
+                        {
+                            uint32_t const e = row[k];
+                            uint32_t const j = e >> 5, sl = e & 31u;
+                            V4 const pj = ld4(rec.pm + j);
+                            T const dx = own.x - (pj.x + T(stencilOff(sl, 0)) * ex);
+                            T const dy = own.y - (pj.y + T(stencilOff(sl, 1)) * ey);
+                            T const dz = own.z - (pj.z + T(stencilOff(sl, 2)) * ez);
+                            T const r2 = dx * dx + dy * dy + dz * dz;
+                            T const r = r2 > T(0) ? r2 * rsqrtT(r2) : T(0);
+                            rho.add(pj.w * kernelW<K, T>(r, hk));
+                        }
+                        rho.fold();
+                    }
+                    double const rhoD = rho.value();
+                    c.cur.rho[t] = rhoD;
+                    c.lists.count[t] = nl;
+                    double Bv[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
+                    double ft[4], fb[4];
+                    derivedRecord(rhoD, c.cur.u[t], Bv, c.cur.psi[t], pa, ft, fb);
+                    rec.ft[t] = mk4<V4>(ft[0], ft[1], ft[2], ft[3]);
+                    rec.fb[t] = mk4<V4>(fb[0], fb[1], fb[2], fb[3]);
+                    chMax = fmax(chMax, ft[2]);
+                }
+            }
+            maxCount = warpMaxU(maxCount);
+            pairs = warpSumU64(pairs);
+            chMax = warpMaxD(chMax);
+            if(lane == 0)
+            {
+                if(maxCount > cap)
+                    atomicMax(&c.status[kStatOverflow], maxCount);
+                atomicMax(&c.status[kStatMaxCount], maxCount);
+                atomicAdd(&c.scal->pairs, pairs);
+                if(!countOnly)
+                    atomicMax(&c.scal->chBits, orderedBits(chMax));
+            }
+        }
+
+        //! Physics variants compiled separately: 0 = the reference's inviscid
+        //! hydro, 1 = hydro + viscosity, 2 = SPMHD (viscosity, Dedner and the
+        //! tensile correction switched at run time).
+        template<int K, typename T, int PH>
+        __global__ void __launch_bounds__(kForceThreads) kForce(DevCtx c, PhysArgs pa)
+        {
+            using V4 = typename PairCfg<T>::V4;
+            Records<V4, T> const rec = records<T>(c);
+            uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+            bool const act = t < c.n && isTarget(c.cur.role[t]);
+            double dtLocal = 1e300;
+            if(act)
+            {
+                bool const av = (PH == 1) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
+                bool const dedner = PH == 2 && (pa.physics & SPH_PHYS_DEDNER);
+                bool const tensile = PH == 2 && (pa.physics & SPH_PHYS_TENSILE);
+                BoxDev const& B = c.boxes[c.cur.box[t]];
+                T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
+                V4 const pi = ld4(rec.pm + t);
+                V4 const vi = ld4(rec.fv + t);
+                V4 const ti = ld4(rec.ft + t);
+                V4 const bi = ld4(rec.fb + t);
+                HConst<T> const hk = hconst<K, T>(vi.w);
+                T const alpha = T(pa.alpha), beta = T(pa.beta), eps = T(pa.avEps);
+                Acc<T> ax, ay, az, D, duav, anx, any, anz, tens, t3x, t3y, t3z, divb, gpx, gpy, gpz;
+                T vsig = ti.z;
+                uint32_t const n = min(c.lists.count[t], c.lists.cap);
+                uint32_t const* row = c.lists.list + size_t(t) * c.lists.cap;
+                for(uint32_t k0 = 0; k0 < n; k0 += kBlock)
+                {
+                    uint32_t const k1 = min(n, k0 + kBlock);
+                    for(uint32_t k = k0; k < k1; ++k)
+                    {
+                        uint32_t const e = row[k];
+                        uint32_t const j = e >> 5, sl = e & 31u;
+                        V4 const pj = ld4(rec.pm + j);
+                        V4 const vj = ld4(rec.fv + j);
+                        V4 const tj = ld4(rec.ft + j);
+                        T const rx = pi.x - (pj.x + T(stencilOff(sl, 0)) * ex);
+                        T const ry = pi.y - (pj.y + T(stencilOff(sl, 1)) * ey);
+                        T const rz = pi.z - (pj.z + T(stencilOff(sl, 2)) * ez);
+                        T const r2 = rx * rx + ry * ry + rz * rz;
+                        T invR = T(0), r = T(0);
+                        if(r2 > T(0))
+                        {
+                            invR = rsqrtT(r2);
+                            r = r2 * invR;
+                        }
+                        T const si = gradWScalar<K, T>(r, invR, hk);
+                        HConst<T> const hkj = hconstFromInv<K, T>(rcpT(vj.w));
+                        T const sj = gradWScalar<K, T>(r, invR, hkj);
+                        T const mj = pj.w;
+                        T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+                        T const vr = vx * rx + vy * ry + vz * rz;
+                        // Isotropic pressure gradient (HydroForces.hpp:155-166).
+                        T const fiso = mj * (ti.y * si + tj.y * sj);
+                        ax.add(-fiso * rx);
+                        ay.add(-fiso * ry);
+                        az.add(-fiso * rz);
+                        // sum m_j s_i v_ij.r: P dV work, div v and the induction term.
+                        T const msi = mj * si;
+                        D.add(msi * vr);
+                        if(av && vr < T(0))
+                        {
+                            T const hb = T(0.5) * (vi.w + vj.w);
+                            T const mu = hb * vr / (r2 + eps * hb * hb);
+                            T const cb = T(0.5) * (ti.z + tj.z);
+                            T const rb = T(0.5) * (ti.x + tj.x);
+                            T const Pi = (-alpha * cb * mu + beta * mu * mu) / rb;
+                            T const g = mj * Pi * T(0.5) * (si + sj);
+                            ax.add(-g * rx);
+                            ay.add(-g * ry);
+                            az.add(-g * rz);
+                            duav.add(T(0.5) * g * vr);
+                        }
+                        T const w = vr * invR;
+                        T const vs = ti.z + tj.z - beta * (w < T(0) ? w : T(0));
+                        vsig = vs > vsig ? vs : vsig;
+                        if constexpr(PH == 2)
+                        {
+                            V4 const bj = ld4(rec.fb + j);
+                            T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
+                            T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
+                            T const ci = msi * Bir * ti.w;
+                            T const cj = mj * sj * Bjr * tj.w;
+                            anx.add(ci * bi.x + cj * bj.x);
+                            any.add(ci * bi.y + cj * bj.y);
+                            anz.add(ci * bi.z + cj * bj.z);
+                            tens.add(ci + cj);
+                            T const wB = msi * Bir;
+                            t3x.add(wB * vx);
+                            t3y.add(wB * vy);
+                            t3z.add(wB * vz);
+                            divb.add(msi * (Bir - Bjr));
+                            if(dedner)
+                            {
+                                T const g = mj * (bi.w * si + bj.w * sj);
+                                gpx.add(g * rx);
+                                gpy.add(g * ry);
+                                gpz.add(g * rz);
+                            }
+                        }
+                    }
+                    ax.fold();
+                    ay.fold();
+                    az.fold();
+                    D.fold();
+                    duav.fold();
+                    if constexpr(PH == 2)
+                    {
+                        anx.fold();
+                        any.fold();
+                        anz.fold();
+                        tens.fold();
+                        t3x.fold();
+                        t3y.fold();
+                        t3z.fold();
+                        divb.fold();
+                        gpx.fold();
+                        gpy.fold();
+                        gpz.fold();
+                    }
+                }
+                // Epilogue in FP64.
+                double const rho = c.cur.rho[t];
+                double const h = c.cur.h[t];
+                double const pr2 = (pa.gamma - 1.0) * c.cur.u[t] / rho; // P_i / rho_i^2
+                double a[3] = {ax.value(), ay.value(), az.value()};
+                double const Dv = D.value();
+                c.d.dudt[t] = pr2 * Dv + duav.value();
+                if constexpr(PH == 2)
+                {
+                    double const Bi[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
+                    double const psi = c.cur.psi[t];
+                    double const an[3] = {anx.value(), any.value(), anz.value()};
+                    double const tsum = tens.value();
+                    double const t3[3] = {t3x.value(), t3y.value(), t3z.value()};
+                    double const gp[3] = {gpx.value(), gpy.value(), gpz.value()};
+                    double const invRho = 1.0 / rho;
+                    double const divB = -invRho * divb.value();
+                    double const divv = -invRho * Dv;
+                    double const ch = __longlong_as_double(static_cast<long long>(c.scal->chBits));
+#pragma unroll
+                    for(int q = 0; q < 3; ++q)
+                    {
+                        a[q] += an[q];
+                        if(tensile)
+                            a[q] -= Bi[q] * tsum;
+                        double dB = -invRho * (t3[q] - Bi[q] * Dv);
+                        if(dedner)
+                            dB -= rho * gp[q];
+                        c.d.dBdt[q][t] = dB;
+                    }
+                    c.d.divB[t] = divB;
+                    c.d.dpsidt[t] = dedner ? (-ch * ch * divB - psi * pa.sigma * ch / h - 0.5 * psi * divv) : 0.0;
+                }
+#pragma unroll
+                for(int q = 0; q < 3; ++q)
+                    c.d.dvdt[q][t] = a[q];
+                double dt = pa.cfl * h / double(vsig);
+                double const amag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+                if(amag > 0.0 && pa.cflForce > 0.0)
+                    dt = fmin(dt, pa.cflForce * sqrt(h / amag));
+                dtLocal = dt;
+            }
+            dtLocal = warpMinD(dtLocal);
+            if((threadIdx.x & 31) == 0 && dtLocal < 1e300)
+                atomicMin(&c.scal->dtBits, orderedBits(dtLocal));
+        }
+
+        template<typename T>
+        constexpr size_t densitySmem()
+        {
+            using V4 = typename PairCfg<T>::V4;
+            return size_t(kDensWarps) * PairCfg<T>::cap * (sizeof(V4) + sizeof(T) + sizeof(uint32_t));
+        }
+
+        template<int K, typename T>
+        void configureK()
+        {
+            cudaFuncSetAttribute(kDensity<K, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(densitySmem<T>()));
+            cudaFuncSetAttribute(kDensity<K, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(densitySmem<T>()));
+        }
+
+        template<int K, typename T, bool PM>
+        void densityOne(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
+        {
+            size_t const smem = densitySmem<T>();
+            uint32_t blocks = (c.cells.ncells + kDensWarps - 1) / kDensWarps;
+            blocks = blocks > 148u * 64u ? 148u * 64u : blocks;
+            if(blocks)
+            {
+                kDensity<K, T, PM><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
+                countLaunches(1);
+            }
+        }
+
+        template<int K, typename T>
+        void densityPM(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
+        {
+            if(pa.cull == SPH_CULL_PAIR_MAX)
+                densityOne<K, T, true>(c, pa, countOnly, s);
+            else
+                densityOne<K, T, false>(c, pa, countOnly, s);
+        }
+
+        template<int K, typename T>
+        void forceOne(DevCtx const& c, PhysArgs const& pa, cudaStream_t s)
+        {
+            unsigned const g = (c.n + kForceThreads - 1) / kForceThreads;
+            if(!g)
+                return;
+            if(pa.physics & SPH_PHYS_MHD)
+            {
+                kForce<K, T, 2><<<g, kForceThreads, 0, s>>>(c, pa);
+                countLaunches(1);
+            }
+            else if(pa.physics & SPH_PHYS_AV)
+            {
+                kForce<K, T, 1><<<g, kForceThreads, 0, s>>>(c, pa);
+                countLaunches(1);
+            }
+            else
+            {
+                kForce<K, T, 0><<<g, kForceThreads, 0, s>>>(c, pa);
+                countLaunches(1);
+            }
+        }
+
+        template<typename T>
+        void densityK(DevCtx const& c, PhysArgs const& pa, int kernel, bool countOnly, cudaStream_t s)
+        {
+            if(kernel == SPH_KERNEL_QUINTIC)
+                densityPM<SPH_KERNEL_QUINTIC, T>(c, pa, countOnly, s);
+            else if(kernel == SPH_KERNEL_WENDLAND_C2)
+                densityPM<SPH_KERNEL_WENDLAND_C2, T>(c, pa, countOnly, s);
+            else
+                densityPM<SPH_KERNEL_CUBIC, T>(c, pa, countOnly, s);
+        }
+
+        template<typename T>
+        void forceK(DevCtx const& c, PhysArgs const& pa, int kernel, cudaStream_t s)
+        {
+            if(kernel == SPH_KERNEL_QUINTIC)
+                forceOne<SPH_KERNEL_QUINTIC, T>(c, pa, s);
+            else if(kernel == SPH_KERNEL_WENDLAND_C2)
+                forceOne<SPH_KERNEL_WENDLAND_C2, T>(c, pa, s);
+            else
+                forceOne<SPH_KERNEL_CUBIC, T>(c, pa, s);
+        }
+    } // namespace
+
+    void configurePairKernels()
+    {
+        static bool done = false;
+        if(done)
+            return;
+        configureK<SPH_KERNEL_CUBIC, float>();
+        configureK<SPH_KERNEL_QUINTIC, float>();
+        configureK<SPH_KERNEL_WENDLAND_C2, float>();
+        configureK<SPH_KERNEL_CUBIC, double>();
+        configureK<SPH_KERNEL_QUINTIC, double>();
+        configureK<SPH_KERNEL_WENDLAND_C2, double>();
+        done = true;
+    }
+
+    void launchDensity(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, bool countOnly, cudaStream_t s)
+    {
+        if(precision == SPH_PREC_FP64)
+            densityK<double>(c, pa, kernel, countOnly, s);
+        else
+            densityK<float>(c, pa, kernel, countOnly, s);
+    }
+
+    void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, cudaStream_t s)
+    {
+        if(precision == SPH_PREC_FP64)
+            forceK<double>(c, pa, kernel, s);
+        else
+            forceK<float>(c, pa, kernel, s);
+    }
+} // namespace sph

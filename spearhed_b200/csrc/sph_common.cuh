@@ -1,0 +1,265 @@
+// Shared device definitions of the B200 SPH step: box/cell-grid descriptors,
+// SPH kernel functions, equation of state, compensated accumulation.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/spearhed_b200.h"
+
+namespace sph
+{
+    // ------------------------------------------------------------------ grid
+    //! One box of the run: the cell grid the neighbour search bins it into.
+    //! Cell edge >= the cull radius on every axis, so the 27-cell stencil holds
+    //! every neighbour (and, on periodic axes, every image within the radius).
+    struct BoxDev
+    {
+        double lo[3];
+        double L[3];
+        double edge[3];
+        float edgef[3];
+        int32_t n[3];
+        int32_t periodic[3];
+        uint32_t cellBase; //!< first global cell id of this box
+        uint32_t ncells;
+    };
+
+    //! Roles (include/spearhed_b200.h, SPH_ROLE_*).
+    __host__ __device__ inline bool isTarget(uint8_t r)
+    {
+        return (r & SPH_ROLE_MOVABLE) && (r & SPH_ROLE_THERMODYNAMIC);
+    }
+    __host__ __device__ inline bool isSource(uint8_t r)
+    {
+        return r & SPH_ROLE_SOURCE;
+    }
+
+    //! Cell coordinate along one axis: floor((x - lo)/edge) clamped to [0, n-1].
+    __device__ __forceinline__ int cellCoord(BoxDev const& b, int a, double x)
+    {
+        double const f = floor((x - b.lo[a]) / b.edge[a]);
+        return f < 0.0 ? 0 : (f >= double(b.n[a]) ? b.n[a] - 1 : int(f));
+    }
+
+    //! Stencil slot 0..26 <-> offset (ox, oy, oz), x fastest; slot 13 is the centre.
+    __host__ __device__ __forceinline__ int stencilOff(int slot, int a)
+    {
+        return a == 0 ? (slot % 3) - 1 : (a == 1 ? ((slot / 3) % 3) - 1 : (slot / 9) - 1);
+    }
+    constexpr int kCentreSlot = 13;
+
+    //! A neighbour-list entry: sorted source index (27 bits) and stencil slot (5 bits).
+    __host__ __device__ __forceinline__ uint32_t packEntry(uint32_t j, uint32_t slot)
+    {
+        return (j << 5) | slot;
+    }
+    constexpr uint32_t kMaxParticles = 1u << 27;
+
+    // --------------------------------------------------------------- kernels
+    // Kernel functions follow the reference's formulas
+    // (include/spearhed/sph/CubicSplineKernel.hpp:49-140,
+    // QuinticSplineKernel.hpp:47-164); the Wendland C2 kernel (support 2h,
+    // W = 21/(16 pi h^3) (1-q/2)^4 (1+2q)) is not in the reference.  Each takes
+    // the reciprocal smoothing length so the pair loop divides nowhere.
+    template<int K>
+    struct Kern;
+
+    template<>
+    struct Kern<SPH_KERNEL_CUBIC>
+    {
+        static constexpr int support = 2;
+        template<typename T>
+        __device__ __forceinline__ static T norm()
+        {
+            return T(0.318309886183790671537767526745028724); // 1/pi
+        }
+        //! W(r,h) h^3 / sigma as a function of x = r/h.
+        template<typename T>
+        __device__ __forceinline__ static T shapeW(T x)
+        {
+            if(x < T(1))
+                return T(1) - T(1.5) * x * x + T(0.75) * x * x * x;
+            if(x < T(2))
+            {
+                T const t = T(2) - x;
+                return T(0.25) * t * t * t;
+            }
+            return T(0);
+        }
+        //! (dW/dr) h^4 / sigma as a function of x = r/h.
+        template<typename T>
+        __device__ __forceinline__ static T shapeDW(T x)
+        {
+            if(x < T(1))
+                return (T(2.25) * x - T(3)) * x;
+            if(x < T(2))
+            {
+                T const t = T(2) - x;
+                return T(-0.75) * t * t;
+            }
+            return T(0);
+        }
+    };
+
+    template<>
+    struct Kern<SPH_KERNEL_QUINTIC>
+    {
+        static constexpr int support = 3;
+        template<typename T>
+        __device__ __forceinline__ static T norm()
+        {
+            return T(0.00265258238486492226281472938954190604); // 1/(120 pi)
+        }
+        template<typename T>
+        __device__ __forceinline__ static T shapeW(T x)
+        {
+            T const a = T(3) - x, b = T(2) - x, c = T(1) - x;
+            T const a2 = a * a, b2 = b * b, c2 = c * c;
+            if(x < T(1))
+                return a2 * a2 * a - T(6) * b2 * b2 * b + T(15) * c2 * c2 * c;
+            if(x < T(2))
+                return a2 * a2 * a - T(6) * b2 * b2 * b;
+            if(x < T(3))
+                return a2 * a2 * a;
+            return T(0);
+        }
+        template<typename T>
+        __device__ __forceinline__ static T shapeDW(T x)
+        {
+            T const a = T(3) - x, b = T(2) - x, c = T(1) - x;
+            T const a2 = a * a, b2 = b * b, c2 = c * c;
+            if(x < T(1))
+                return T(-5) * a2 * a2 + T(30) * b2 * b2 - T(75) * c2 * c2;
+            if(x < T(2))
+                return T(-5) * a2 * a2 + T(30) * b2 * b2;
+            if(x < T(3))
+                return T(-5) * a2 * a2;
+            return T(0);
+        }
+    };
+
+    template<>
+    struct Kern<SPH_KERNEL_WENDLAND_C2>
+    {
+        static constexpr int support = 2;
+        template<typename T>
+        __device__ __forceinline__ static T norm()
+        {
+            return T(0.417781725616225256392384879024100200); // 21/(16 pi)
+        }
+        template<typename T>
+        __device__ __forceinline__ static T shapeW(T x)
+        {
+            if(x < T(2))
+            {
+                T const t = T(1) - T(0.5) * x;
+                T const t2 = t * t;
+                return t2 * t2 * (T(1) + T(2) * x);
+            }
+            return T(0);
+        }
+        //! dW/dr h^4 / sigma = -5 x (1-x/2)^3.
+        template<typename T>
+        __device__ __forceinline__ static T shapeDW(T x)
+        {
+            if(x < T(2))
+            {
+                T const t = T(1) - T(0.5) * x;
+                return T(-5) * x * t * t * t;
+            }
+            return T(0);
+        }
+    };
+
+    //! Per-particle kernel constants: 1/h, sigma/h^3, sigma/h^4.
+    template<typename T>
+    struct HConst
+    {
+        T invh, wnorm, dwnorm;
+    };
+    template<int K, typename T>
+    __device__ __forceinline__ HConst<T> hconstFromInv(T ih)
+    {
+        T const ih3 = ih * ih * ih;
+        T const w = Kern<K>::template norm<T>() * ih3;
+        return HConst<T>{ih, w, w * ih};
+    }
+    template<int K, typename T>
+    __device__ __forceinline__ HConst<T> hconst(T h)
+    {
+        return hconstFromInv<K, T>(T(1) / h);
+    }
+
+    //! W(r, h).
+    template<int K, typename T>
+    __device__ __forceinline__ T kernelW(T r, HConst<T> const& c)
+    {
+        return c.wnorm * Kern<K>::shapeW(r * c.invh);
+    }
+
+    //! gradWScalar(r, invR, h) = dW/dr(r, h) * invR: zero when r is not > 0 or
+    //! r >= support h (CubicSplineKernel.hpp:183-192).
+    template<int K, typename T>
+    __device__ __forceinline__ T gradWScalar(T r, T invR, HConst<T> const& c)
+    {
+        T const x = r * c.invh;
+        if(!(r > T(0)) || x >= T(Kern<K>::support))
+            return T(0);
+        return c.dwnorm * Kern<K>::shapeDW(x) * invR;
+    }
+
+    // ------------------------------------------------------------------- EOS
+    //! P = (gamma - 1) rho u (EquationOfState.hpp:32-35).
+    template<typename T>
+    __device__ __forceinline__ T pressure(T gamma, T rho, T u)
+    {
+        return (gamma - T(1)) * rho * u;
+    }
+
+    // -------------------------------------------------- compensated summation
+    //! Knuth's TwoSum: s + e == a + b exactly.
+    __device__ __forceinline__ void twoSum(float a, float b, float& s, float& e)
+    {
+        s = __fadd_rn(a, b);
+        float const bb = __fsub_rn(s, a);
+        e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+    }
+
+    //! FP32 accumulator with a running compensation term.  Terms are summed
+    //! plainly into a short block partial, and each block partial is folded
+    //! into (hi, lo) with TwoSum, so the error no longer grows with the
+    //! neighbour count (a block of up to 8 terms costs one FP32 rounding each).
+    struct CompAcc
+    {
+        float hi = 0.f, lo = 0.f;
+        __device__ __forceinline__ void fold(float part)
+        {
+            float s, e;
+            twoSum(hi, part, s, e);
+            hi = s;
+            lo += e;
+        }
+        __device__ __forceinline__ double value() const
+        {
+            return double(hi) + double(lo);
+        }
+    };
+
+    //! Ordered-integer view of a non-negative double, for atomicMax/atomicMin.
+    __device__ __forceinline__ unsigned long long orderedBits(double x)
+    {
+        return static_cast<unsigned long long>(__double_as_longlong(x));
+    }
+
+    // ----------------------------------------------------------- status word
+    //! Device status words the host reads after every call.
+    enum StatusWord
+    {
+        kStatOverflow = 0,   //!< largest neighbour count that did not fit the list
+        kStatOutside = 1,    //!< particles found outside a non-periodic box
+        kStatNonFinite = 2,  //!< non-finite positions
+        kStatMaxCount = 3,   //!< largest neighbour count seen (list sizing)
+        kStatWords = 8
+    };
+} // namespace sph

@@ -1,0 +1,526 @@
+// Per-particle kernels of the step: drift + cell keys, cell ranges, permute +
+// record packing, kick + conserved-quantity partial sums, finalisation.
+//
+// These replace the reference's per-particle launches (launchForEach over
+// PushVelocity / EulerIntegrate, spmacc/particles/algorithms/LaunchForEach.hpp:129-160;
+// include/spearhed/particles/pusher/PushVelocity.hpp:38-41, EulerIntegrate.hpp:45-51)
+// and its region bookkeeping.  All are HBM-streaming kernels: coalesced FP64
+// columns in, coalesced columns out.
+#include "sph_launch.hpp"
+
+#include <cfloat>
+
+namespace sph
+{
+    namespace
+    {
+        constexpr int kThreads = 256;
+
+        //! Drift (Movable): x += v dt with periodic wrap; then the cell key.
+        //! Key = 2 * global cell + (0 for targets, 1 for other sources); particles
+        //! that are no source sort behind every cell (key 2 * ncells).
+        __global__ void __launch_bounds__(kThreads) kDriftKeys(DevCtx c, bool drift)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p >= c.n)
+                return;
+            uint8_t const role = c.cur.role[p];
+            BoxDev const& B = c.boxes[c.cur.box[p]];
+            double const dt = c.scal->dt;
+            double x[3];
+            bool finite = true;
+#pragma unroll
+            for(int a = 0; a < 3; ++a)
+            {
+                x[a] = c.cur.x[a][p];
+                if(drift && (role & SPH_ROLE_MOVABLE))
+                {
+                    x[a] += c.cur.v[a][p] * dt;
+                    if(B.periodic[a])
+                    {
+                        double const hiEdge = B.lo[a] + B.L[a];
+                        for(int it = 0; it < 4 && x[a] >= hiEdge; ++it)
+                            x[a] -= B.L[a];
+                        for(int it = 0; it < 4 && x[a] < B.lo[a]; ++it)
+                            x[a] += B.L[a];
+                    }
+                    c.cur.x[a][p] = x[a];
+                }
+                finite = finite && isfinite(x[a]);
+            }
+            uint32_t key = 2u * c.cells.ncells;
+            if(!finite)
+            {
+                atomicAdd(&c.status[kStatNonFinite], 1u);
+            }
+            else
+            {
+                bool outside = false;
+#pragma unroll
+                for(int a = 0; a < 3; ++a)
+                    if(!B.periodic[a] && (x[a] < B.lo[a] || x[a] > B.lo[a] + B.L[a]))
+                        outside = true;
+                if(outside)
+                    atomicAdd(&c.status[kStatOutside], 1u);
+                if(isSource(role))
+                {
+                    int const cx = cellCoord(B, 0, x[0]);
+                    int const cy = cellCoord(B, 1, x[1]);
+                    int const cz = cellCoord(B, 2, x[2]);
+                    uint32_t const cell = B.cellBase + (uint32_t(cz) * uint32_t(B.n[1]) + uint32_t(cy)) * uint32_t(B.n[0])
+                                          + uint32_t(cx);
+                    key = 2u * cell + (isTarget(role) ? 0u : 1u);
+                }
+            }
+            c.keysA[p] = key;
+            c.valsA[p] = p;
+        }
+
+        __global__ void __launch_bounds__(kThreads) kCellRanges(uint32_t const* __restrict__ keys, uint32_t n, Cells cells)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p >= n)
+                return;
+            uint32_t const k = keys[p];
+            uint32_t const cell = k >> 1;
+            if(cell >= cells.ncells)
+                return;
+            uint32_t const other = k & 1u;
+            uint32_t const kp = p > 0 ? keys[p - 1] : 0xffffffffu;
+            uint32_t const kn = p + 1 < n ? keys[p + 1] : 0xffffffffu;
+            bool const firstOfCell = p == 0 || (kp >> 1) != cell;
+            bool const lastOfCell = p + 1 == n || (kn >> 1) != cell;
+            if(firstOfCell)
+                cells.start[cell] = p;
+            if(other && (p == 0 || kp != k))
+                cells.mid[cell] = p;
+            if(lastOfCell)
+            {
+                cells.end[cell] = p + 1;
+                if(!other)
+                    cells.mid[cell] = p + 1;
+            }
+        }
+
+        template<typename V4, typename T>
+        __global__ void __launch_bounds__(kThreads)
+            kPermute(DevCtx c, uint32_t const* __restrict__ perm, PhysArgs pa, Records<V4, T> rec)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p >= c.n)
+                return;
+            uint32_t const q = perm[p];
+            double x[3], v[3], Bv[3];
+#pragma unroll
+            for(int a = 0; a < 3; ++a)
+            {
+                x[a] = c.cur.x[a][q];
+                v[a] = c.cur.v[a][q];
+                Bv[a] = c.cur.B[a][q];
+                c.alt.x[a][p] = x[a];
+                c.alt.v[a][p] = v[a];
+                c.alt.B[a][p] = Bv[a];
+            }
+            double const u = c.cur.u[q], m = c.cur.m[q], h = c.cur.h[q], rho = c.cur.rho[q], psi = c.cur.psi[q];
+            c.alt.u[p] = u;
+            c.alt.m[p] = m;
+            c.alt.h[p] = h;
+            c.alt.rho[p] = rho;
+            c.alt.psi[p] = psi;
+            c.alt.id[p] = c.cur.id[q];
+            int32_t const b = c.cur.box[q];
+            c.alt.box[p] = b;
+            uint8_t const role = c.cur.role[q];
+            c.alt.role[p] = role;
+            if(!isSource(role))
+                return;
+            BoxDev const& B = c.boxes[b];
+            double rel[3];
+#pragma unroll
+            for(int a = 0; a < 3; ++a)
+            {
+                int const ca = cellCoord(B, a, x[a]);
+                rel[a] = x[a] - (B.lo[a] + double(ca) * B.edge[a]);
+            }
+            rec.pm[p] = mk4<V4>(rel[0], rel[1], rel[2], m);
+            rec.hc[p] = T(h);
+            rec.fv[p] = mk4<V4>(v[0], v[1], v[2], h);
+            if(!isTarget(role))
+            {
+                // Frozen source (Boundary species): rho and u keep their initial values.
+                double ft[4], fb[4];
+                derivedRecord(rho, u, Bv, psi, pa, ft, fb);
+                rec.ft[p] = mk4<V4>(ft[0], ft[1], ft[2], ft[3]);
+                rec.fb[p] = mk4<V4>(fb[0], fb[1], fb[2], fb[3]);
+            }
+        }
+
+        __device__ __forceinline__ double warpSum(double v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v += __shfl_down_sync(0xffffffffu, v, o);
+            return v;
+        }
+        __device__ __forceinline__ double warpMax(double v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+            return v;
+        }
+
+        //! Kick (Movable & Thermodynamic): v += dvdt dt, u += dudt dt, and with MHD
+        //! B += dBdt dt, psi += dpsidt dt; then FP64 block partial sums of the
+        //! conserved quantities of the new state (deterministic: fixed order).
+        __global__ void __launch_bounds__(kThreads) kKick(DevCtx c, PhysArgs pa)
+        {
+            __shared__ double red[kThreads / 32][kDiagWords];
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            double acc[kDiagWords];
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+                acc[k] = 0.0;
+            bool const mhd = pa.physics & SPH_PHYS_MHD;
+            if(p < c.n && isTarget(c.cur.role[p]))
+            {
+                double const dt = c.scal->dt;
+                double const m = c.cur.m[p];
+                double v2 = 0.0, B2 = 0.0;
+#pragma unroll
+                for(int a = 0; a < 3; ++a)
+                {
+                    double const va = c.cur.v[a][p] + c.d.dvdt[a][p] * dt;
+                    c.cur.v[a][p] = va;
+                    v2 += va * va;
+                    acc[3 + a] = m * va;
+                }
+                double const u = c.cur.u[p] + c.d.dudt[p] * dt;
+                c.cur.u[p] = u;
+                if(mhd)
+                {
+#pragma unroll
+                    for(int a = 0; a < 3; ++a)
+                    {
+                        double const Ba = c.cur.B[a][p] + c.d.dBdt[a][p] * dt;
+                        c.cur.B[a][p] = Ba;
+                        B2 += Ba * Ba;
+                    }
+                    c.cur.psi[p] += c.d.dpsidt[p] * dt;
+                }
+                acc[0] = 0.5 * m * v2;
+                acc[1] = m * u;
+                double const rho = c.cur.rho[p];
+                acc[2] = (mhd && rho > 0.0) ? 0.5 * m * B2 / (pa.mu0 * rho) : 0.0;
+                if(mhd && B2 > 0.0)
+                {
+                    double const e = fabs(c.d.divB[p]) * c.cur.h[p] / sqrt(B2);
+                    acc[6] = e;
+                    acc[7] = 1.0;
+                    acc[8] = e;
+                }
+                acc[9] = 1.0;
+            }
+            int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+            {
+                double const r = (k == 8) ? warpMax(acc[k]) : warpSum(acc[k]);
+                if(lane == 0)
+                    red[warp][k] = r;
+            }
+            __syncthreads();
+            if(threadIdx.x < kDiagWords)
+            {
+                int const k = threadIdx.x;
+                double r = 0.0;
+                for(int w = 0; w < kThreads / 32; ++w)
+                    r = (k == 8) ? fmax(r, red[w][k]) : r + red[w][k];
+                c.partials[size_t(blockIdx.x) * kDiagWords + k] = r;
+            }
+        }
+
+        //! Sums the block partials in a fixed order and advances time (and the
+        //! CFL dt when enabled).
+        __global__ void __launch_bounds__(kThreads) kFinalize(DevCtx c, bool cfl)
+        {
+            __shared__ double red[kThreads][kDiagWords];
+            double acc[kDiagWords];
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+                acc[k] = 0.0;
+            for(uint32_t b = threadIdx.x; b < c.nPartialBlocks; b += kThreads)
+#pragma unroll
+                for(int k = 0; k < kDiagWords; ++k)
+                    acc[k] = (k == 8) ? fmax(acc[k], c.partials[size_t(b) * kDiagWords + k])
+                                      : acc[k] + c.partials[size_t(b) * kDiagWords + k];
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+                red[threadIdx.x][k] = acc[k];
+            __syncthreads();
+            for(int s = kThreads / 2; s > 0; s >>= 1)
+            {
+                if(int(threadIdx.x) < s)
+#pragma unroll
+                    for(int k = 0; k < kDiagWords; ++k)
+                        red[threadIdx.x][k] = (k == 8) ? fmax(red[threadIdx.x][k], red[threadIdx.x + s][k])
+                                                       : red[threadIdx.x][k] + red[threadIdx.x + s][k];
+                __syncthreads();
+            }
+            if(threadIdx.x == 0)
+            {
+                StepScalars& S = *c.scal;
+                double const dt = S.dt;
+                S.time += dt;
+                S.steps += 1;
+                S.pairsAccum += double(S.pairs);
+#pragma unroll
+                for(int k = 0; k < 10; ++k)
+                    c.diag[k] = red[0][k];
+                c.diag[10] = dt;
+                c.diag[11] = S.time;
+                if(cfl)
+                {
+                    double const dtn = __longlong_as_double(static_cast<long long>(S.dtBits));
+                    if(dtn > 0.0 && dtn < 1e300)
+                        S.dt = dtn;
+                }
+            }
+        }
+
+        __global__ void kUnpermute(uint32_t n, uint32_t const* __restrict__ id, double const* __restrict__ src, double* __restrict__ dst)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p < n)
+                dst[id[p]] = src[p];
+        }
+        __global__ void kUnpermuteInt(uint32_t n, uint32_t const* __restrict__ id, uint32_t const* __restrict__ src, int32_t* __restrict__ dst)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p < n)
+                dst[id[p]] = int32_t(src[p]);
+        }
+        //! master[p] = src[id[p]] (or dflt) for the particles of one species
+        //! (ids in [off, off + cnt)); src is in input order.
+        __global__ void kGatherSpecies(
+            uint32_t n,
+            uint32_t const* __restrict__ id,
+            uint32_t off,
+            uint32_t cnt,
+            double const* __restrict__ src,
+            double dflt,
+            double* __restrict__ master)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p >= n)
+                return;
+            uint32_t const i = id[p];
+            if(i - off < cnt)
+                master[p] = src ? src[i] : dflt;
+        }
+        __global__ void kGatherSpeciesInt(
+            uint32_t n,
+            uint32_t const* __restrict__ id,
+            uint32_t off,
+            uint32_t cnt,
+            int32_t const* __restrict__ src,
+            int32_t* __restrict__ master)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            if(p >= n)
+                return;
+            uint32_t const i = id[p];
+            if(i - off < cnt)
+                master[p] = src[i];
+        }
+        __global__ void kFill(double* p, size_t n, double v)
+        {
+            size_t const i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if(i < n)
+                p[i] = v;
+        }
+
+        //! Per-box conserved sums: one block per box over its cells' targets.
+        __global__ void __launch_bounds__(kThreads) kBoxReduce(DevCtx c, PhysArgs pa, double* out)
+        {
+            __shared__ double red[kThreads / 32][kDiagWords];
+            BoxDev const& B = c.boxes[blockIdx.x];
+            bool const mhd = pa.physics & SPH_PHYS_MHD;
+            double acc[kDiagWords];
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+                acc[k] = 0.0;
+            for(uint32_t lc = 0; lc < B.ncells; ++lc)
+            {
+                uint32_t const cell = B.cellBase + lc;
+                uint32_t const s = c.cells.start[cell], e = c.cells.mid[cell];
+                for(uint32_t p = s + threadIdx.x; p < e; p += kThreads)
+                {
+                    double const m = c.cur.m[p];
+                    double v2 = 0.0, B2 = 0.0;
+                    for(int a = 0; a < 3; ++a)
+                    {
+                        double const va = c.cur.v[a][p];
+                        v2 += va * va;
+                        acc[3 + a] += m * va;
+                        if(mhd)
+                            B2 += c.cur.B[a][p] * c.cur.B[a][p];
+                    }
+                    acc[0] += 0.5 * m * v2;
+                    acc[1] += m * c.cur.u[p];
+                    if(mhd && c.cur.rho[p] > 0.0)
+                        acc[2] += 0.5 * m * B2 / (pa.mu0 * c.cur.rho[p]);
+                    if(mhd && B2 > 0.0)
+                    {
+                        double const e2 = fabs(c.d.divB[p]) * c.cur.h[p] / sqrt(B2);
+                        acc[6] += e2;
+                        acc[7] += 1.0;
+                        acc[8] = fmax(acc[8], e2);
+                    }
+                    acc[9] += 1.0;
+                }
+            }
+            int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+            {
+                double const r = (k == 8) ? warpMax(acc[k]) : warpSum(acc[k]);
+                if(lane == 0)
+                    red[warp][k] = r;
+            }
+            __syncthreads();
+            if(threadIdx.x < kDiagWords)
+            {
+                int const k = threadIdx.x;
+                double r = 0.0;
+                for(int w = 0; w < kThreads / 32; ++w)
+                    r = (k == 8) ? fmax(r, red[w][k]) : r + red[w][k];
+                out[size_t(blockIdx.x) * kDiagWords + k] = r;
+            }
+        }
+    } // namespace
+
+    uint32_t partialBlocks(uint32_t n)
+    {
+        return (n + kThreads - 1) / kThreads;
+    }
+
+    void launchDriftKeys(DevCtx const& c, bool drift, cudaStream_t s)
+    {
+        if(c.n)
+        {
+            kDriftKeys<<<(c.n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, drift);
+            countLaunches(1);
+        }
+    }
+
+    void launchCellRanges(DevCtx const& c, uint32_t const* sortedKeys, cudaStream_t s)
+    {
+        cudaMemsetAsync(c.cells.start, 0, size_t(c.cells.ncells) * 4, s);
+        cudaMemsetAsync(c.cells.mid, 0, size_t(c.cells.ncells) * 4, s);
+        cudaMemsetAsync(c.cells.end, 0, size_t(c.cells.ncells) * 4, s);
+        if(c.n)
+        {
+            kCellRanges<<<(c.n + kThreads - 1) / kThreads, kThreads, 0, s>>>(sortedKeys, c.n, c.cells);
+            countLaunches(1);
+        }
+    }
+
+    void launchPermute(DevCtx const& c, uint32_t const* perm, PhysArgs const& pa, int precision, cudaStream_t s)
+    {
+        if(!c.n)
+            return;
+        unsigned const g = (c.n + kThreads - 1) / kThreads;
+        if(precision == SPH_PREC_FP64)
+        {
+            kPermute<D4, double><<<g, kThreads, 0, s>>>(c, perm, pa, c.r64);
+            countLaunches(1);
+        }
+        else
+        {
+            kPermute<float4, float><<<g, kThreads, 0, s>>>(c, perm, pa, c.r32);
+            countLaunches(1);
+        }
+    }
+
+    void launchKick(DevCtx const& c, PhysArgs const& pa, cudaStream_t s)
+    {
+        if(c.n)
+        {
+            kKick<<<partialBlocks(c.n), kThreads, 0, s>>>(c, pa);
+            countLaunches(1);
+        }
+    }
+
+    void launchFinalize(DevCtx const& c, bool cfl, cudaStream_t s)
+    {
+        kFinalize<<<1, kThreads, 0, s>>>(c, cfl);
+        countLaunches(1);
+    }
+
+    void launchUnpermute(uint32_t n, uint32_t const* id, double const* src, double* dst, cudaStream_t s)
+    {
+        if(n)
+        {
+            kUnpermute<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, src, dst);
+            countLaunches(1);
+        }
+    }
+
+    void launchUnpermuteInt(uint32_t n, uint32_t const* id, uint32_t const* src, int32_t* dst, cudaStream_t s)
+    {
+        if(n)
+        {
+            kUnpermuteInt<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, src, dst);
+            countLaunches(1);
+        }
+    }
+
+    void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, cudaStream_t s)
+    {
+        kBoxReduce<<<c.nbox, kThreads, 0, s>>>(c, pa, out);
+        countLaunches(1);
+    }
+
+    void launchGatherSpecies(
+        uint32_t n,
+        uint32_t const* id,
+        uint32_t off,
+        uint32_t cnt,
+        double const* src,
+        double dflt,
+        double* master,
+        cudaStream_t s)
+    {
+        if(n)
+        {
+            kGatherSpecies<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, dflt, master);
+            countLaunches(1);
+        }
+    }
+
+    void launchGatherSpeciesInt(
+        uint32_t n,
+        uint32_t const* id,
+        uint32_t off,
+        uint32_t cnt,
+        int32_t const* src,
+        int32_t* master,
+        cudaStream_t s)
+    {
+        if(n)
+        {
+            kGatherSpeciesInt<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, master);
+            countLaunches(1);
+        }
+    }
+
+    void launchFill(double* p, size_t n, double v, cudaStream_t s)
+    {
+        if(n)
+        {
+            kFill<<<unsigned((n + 255) / 256), 256, 0, s>>>(p, n, v);
+            countLaunches(1);
+        }
+    }
+} // namespace sph

@@ -103,7 +103,7 @@ def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False):
                     meta={"n_left": left.shape[1], "n_right": right.shape[1], "dx_left": dxl, "dx_right": dxr})
 
 
-def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45):
+def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, jitter=0.0, seed=2):
     """Orszag-Tang vortex in a thin periodic slab [0,1]^2 x [0, nz/nx].
 
     nx x nx x nz lattice of equal-mass particles; rho = 25/(36 pi), P = 5/(12 pi),
@@ -111,11 +111,18 @@ def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45):
     Wendland C2 with h = hfact x spacing (hfact 1.45: 92 lattice neighbours,
     ~102 in the continuum), AV, SPMHD with Dedner cleaning and the tensile
     correction, CFL time step.  nx = 512, nz = 4 gives N = 1,048,576.
+    ``jitter`` > 0 displaces every particle uniformly by up to jitter x spacing
+    per axis (Philox, key ``seed``); the benchmark workload uses none.
     """
     gamma = 5.0 / 3.0
     dx = 1.0 / nx
     Lz = nz * dx
     pos = lattice((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (nx, nx, nz))
+    if jitter > 0.0:
+        pos = pos + jitter * dx * philox_uniform(seed, pos.shape)
+        pos[0] %= 1.0
+        pos[1] %= 1.0
+        pos[2] %= Lz
     n = pos.shape[1]
     s = abi.Species(n)
     s.pos[:] = pos
