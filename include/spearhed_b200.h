@@ -235,6 +235,26 @@ int sph_get_timings(sph_ctx* ctx, int32_t n, double* ms);
  * replay it (on = 1) or launch the kernels one by one (on = 0, the default). */
 int sph_use_graph(sph_ctx* ctx, int32_t on);
 
+/* Density summation that allocates no device memory, for callers that cannot
+ * call cudaMalloc (no counterpart in the reference).
+ *
+ * Some callers cannot allocate: a host framework that owns all device memory
+ * through its own pool, code running where an allocation would synchronise the
+ * device, or a plugin hosted by a program that forbids the CUDA allocator.  This
+ * entry point takes caller-owned DEVICE arrays (positions, mass, h; length n) and
+ * writes rho (device, length n, input order); its scratch is one fixed 32 MiB
+ * device array inside this library (held on every GPU that loads it until the
+ * process exits).  Limits: n <= 262144 particles, <= 262144 cells, one box,
+ * params->cull == SPH_CULL_GLOBAL; larger inputs return SPH_ERR_INVALID.
+ * Every Default-species rule applies (all particles are targets and sources).
+ * The work runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * the call returns after it finished.  Calls share the scratch array: calls
+ * whose device work overlaps (other threads or unordered streams) race and give
+ * wrong results.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. */
+int sph_density_noalloc(const SphParams* params, const SphBox* box, int64_t n, const double* x, const double* y,
+                        const double* z, const double* mass, const double* h, double* rho, void* stream);
+
 const char* sph_last_error_string(void);
 
 #ifdef __cplusplus

@@ -138,6 +138,15 @@ namespace
     }
 } // namespace
 
+namespace sph
+{
+    //! Records the message sph_last_error_string() returns on this thread.
+    int recordError(int code, std::string msg)
+    {
+        return fail(code, std::move(msg));
+    }
+} // namespace sph
+
 struct sph_ctx
 {
     SphParams p{};
