@@ -165,6 +165,7 @@ struct sph_ctx
     sph::PhysArgs pa{};
     std::vector<void*> allocs;
     double* boxOut = nullptr;
+    double* boxScratch = nullptr;
     std::vector<double*> staging;
     bool useGraph = false;
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
@@ -202,6 +203,7 @@ struct sph_ctx
         staging.clear();
         dc = sph::DevCtx{};
         boxOut = nullptr;
+        boxScratch = nullptr;
         allocated = false;
         deviceCurrent = false;
         densityValid = false;
@@ -476,7 +478,8 @@ int sph_ctx::allocate()
         return st;
     dc.nPartialBlocks = sph::partialBlocks(n);
     if((st = alloc(dc.partials, size_t(dc.nPartialBlocks) * sph::kDiagWords))
-       || (st = alloc(boxOut, size_t(nbox) * sph::kDiagWords)) || (st = alloc(dc.lists.count, n)))
+       || (st = alloc(boxOut, size_t(nbox) * sph::kDiagWords))
+       || (st = alloc(boxScratch, sph::boxReduceScratchDoubles(nbox))) || (st = alloc(dc.lists.count, n)))
         return st;
     SPH_CUDA_TRY(cudaMemsetAsync(dc.diag, 0, sizeof(double) * sph::kDiagWords, stream));
     dc.keyBits = 1;
@@ -1096,7 +1099,7 @@ namespace
         int st = ctx->ensureDevice();
         if(st)
             return st;
-        sph::launchBoxReduce(ctx->dc, ctx->pa, ctx->boxOut, ctx->stream);
+        sph::launchBoxReduce(ctx->dc, ctx->pa, ctx->boxOut, ctx->boxScratch, ctx->stream);
         perBox.resize(size_t(ctx->dc.nbox) * sph::kDiagWords);
         SPH_CUDA_TRY(cudaMemcpyAsync(perBox.data(), ctx->boxOut, perBox.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
         SPH_CUDA_TRY(cudaMemcpyAsync(&sc, ctx->dc.scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));

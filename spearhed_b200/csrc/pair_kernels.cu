@@ -32,6 +32,7 @@ namespace sph
     {
         constexpr int kDensWarps = 4;
         constexpr int kForceThreads = 128;
+        constexpr int kForceMinBlocks = 5; //!< FP32: caps registers near 100 per thread (20 warps per SM)
         constexpr int kBlock = 8; //!< terms per compensated block
 
         template<typename T>
@@ -40,13 +41,13 @@ namespace sph
         struct PairCfg<float>
         {
             using V4 = float4;
-            static constexpr int cap = 1024;
+            static constexpr int cap = 256;
         };
         template<>
         struct PairCfg<double>
         {
             using V4 = D4;
-            static constexpr int cap = 512;
+            static constexpr int cap = 256;
         };
 
         template<typename T>
@@ -185,11 +186,29 @@ namespace sph
             return v;
         }
 
+        //! Lanes per target for a chunk of nt targets (power of two, nt * S <= 32):
+        //! a full chunk gives every lane its own target; a short chunk spreads each
+        //! target over S lanes that sweep interleaved candidates.
+        __device__ __forceinline__ int subLanes(uint32_t nt)
+        {
+            return nt > 16 ? 1 : (nt > 8 ? 2 : (nt > 4 ? 4 : (nt > 2 ? 8 : (nt > 1 ? 16 : 32))));
+        }
+
+        //! Compensated-sum combine of two (hi, lo) partials (TwoSum on the heads).
+        __device__ __forceinline__ void combineComp(float& hi, float& lo, float ohi, float olo)
+        {
+            float s, e;
+            twoSum(hi, ohi, s, e);
+            hi = s;
+            lo = lo + olo + e;
+        }
+
         template<int K, typename T, bool PAIRMAX>
         __global__ void __launch_bounds__(kDensWarps * 32) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
         {
             using V4 = typename PairCfg<T>::V4;
             constexpr int CAP = PairCfg<T>::cap;
+            constexpr int U = 4; //!< candidates per lane per cull iteration (independent chains)
             extern __shared__ __align__(32) unsigned char smem[];
             int const warp = threadIdx.x >> 5;
             int const lane = threadIdx.x & 31;
@@ -258,11 +277,19 @@ namespace sph
                 }
                 uint32_t const pre = incl - sCnt;
                 uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+                T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
 
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 32)
                 {
-                    uint32_t const t = tc + uint32_t(lane);
-                    bool const act = t < tEnd;
+                    uint32_t const nt = min(32u, tEnd - tc);
+                    int const S = subLanes(nt);
+                    int const sub = lane & (S - 1);
+                    uint32_t const tt = uint32_t(lane) / uint32_t(S);
+                    uint32_t const groupBase = tt * uint32_t(S);
+                    uint32_t const groupMask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << groupBase);
+                    uint32_t const subBelow = (1u << sub) - 1u;
+                    bool const act = tt < nt;
+                    uint32_t const t = tc + tt;
                     V4 own{};
                     T hi = T(1);
                     if(act)
@@ -272,7 +299,7 @@ namespace sph
                     }
                     uint32_t const selfEnt = packEntry(t, kCentreSlot);
                     uint32_t* row = c.lists.list + size_t(t) * cap;
-                    uint32_t nl = 0;
+                    uint32_t nl = 0; // same value on every lane of the target's group
                     for(uint32_t cb = 0; cb < total; cb += CAP)
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
@@ -301,12 +328,21 @@ namespace sph
                             }
                         }
                         __syncwarp();
-                        if(act)
+                        uint32_t const m = ce - cb;
+                        // The warp walks candidates in order; lane (tt, sub) tests
+                        // candidates q = q0 + u*S + sub.  Accepted entries keep the
+                        // candidate order in the row.
+                        for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(U * S))
                         {
-                            uint32_t const m = ce - cb;
-                            for(uint32_t q = 0; q < m; ++q)
+                            bool accU[U];
+                            uint32_t entU[U];
+#pragma unroll
+                            for(int u = 0; u < U; ++u)
                             {
-                                V4 const pj = sPos[q];
+                                uint32_t const q = q0 + uint32_t(u * S + sub);
+                                bool ok = act && q < m;
+                                uint32_t const qq = ok ? q : 0u;
+                                V4 const pj = sPos[qq];
                                 T const dx = subRn(own.x, pj.x);
                                 T const dy = subRn(own.y, pj.y);
                                 T const dz = subRn(own.z, pj.z);
@@ -314,38 +350,59 @@ namespace sph
                                 T R2 = R2g;
                                 if constexpr(PAIRMAX)
                                 {
-                                    T const hj = sH[q];
+                                    T const hj = sH[qq];
                                     T const R = mulRn(supT, hi > hj ? hi : hj);
                                     R2 = mulRn(R, R);
                                 }
-                                if(r2 < R2)
-                                {
-                                    uint32_t const e = sEnt[q];
-                                    if(e != selfEnt)
+                                entU[u] = sEnt[qq];
+                                accU[u] = ok && r2 < R2 && entU[u] != selfEnt;
+                            }
+                            if(S == 1)
+                            {
+#pragma unroll
+                                for(int u = 0; u < U; ++u)
+                                    if(accU[u])
                                     {
                                         if(!countOnly && nl < cap)
-                                            row[nl] = e;
+                                            row[nl] = entU[u];
                                         ++nl;
                                     }
+                            }
+                            else
+                            {
+#pragma unroll
+                                for(int u = 0; u < U; ++u)
+                                {
+                                    uint32_t const bits = __ballot_sync(0xffffffffu, accU[u]) & groupMask;
+                                    if(accU[u])
+                                    {
+                                        uint32_t const k = nl + __popc((bits >> groupBase) & subBelow);
+                                        if(!countOnly && k < cap)
+                                            row[k] = entU[u];
+                                    }
+                                    nl += __popc(bits);
                                 }
                             }
                         }
                     }
-                    maxCount = max(maxCount, act ? nl : 0u);
-                    pairs += act ? nl : 0u;
-                    if(countOnly || !act)
+                    bool const lead = act && sub == 0;
+                    maxCount = max(maxCount, lead ? nl : 0u);
+                    pairs += lead ? nl : 0u;
+                    if(countOnly)
                         continue;
+                    __syncwarp();
                     // Density over the compact row (DensitySummation.hpp:57-93):
-                    // rho_i = m_i W(0, h_i) + sum_j m_j W(r_ij, h_i).
-                    uint32_t const n = min(nl, cap);
+                    // rho_i = m_i W(0, h_i) + sum_j m_j W(r_ij, h_i); the S lanes of a
+                    // target take every S-th entry and their partials are combined.
+                    uint32_t const n = act ? min(nl, cap) : 0u;
                     HConst<T> const hk = hconst<K, T>(hi);
                     Acc<T> rho;
-                    rho.add(own.w * kernelW<K, T>(T(0), hk));
-                    T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
-                    for(uint32_t k0 = 0; k0 < n; k0 += kBlock)
+                    if(lead)
+                        rho.add(own.w * kernelW<K, T>(T(0), hk));
+                    uint32_t k = uint32_t(sub);
+                    while(k < n)
                     {
-                        uint32_t const k1 = min(n, k0 + kBlock);
-                        for(uint32_t k = k0; k < k1; ++k)
+                        for(int b = 0; b < kBlock && k < n; ++b, k += uint32_t(S))
                         {
                             uint32_t const e = row[k];
                             uint32_t const j = e >> 5, sl = e & 31u;
@@ -359,7 +416,28 @@ namespace sph
                         }
                         rho.fold();
                     }
-                    double const rhoD = rho.value();
+                    rho.fold();
+                    double rhoD;
+                    if constexpr(sizeof(T) == 4)
+                    {
+                        float rh = rho.c.hi, rl = rho.c.lo;
+                        for(int off = S >> 1; off > 0; off >>= 1)
+                        {
+                            float const oh = __shfl_down_sync(0xffffffffu, rh, off, S);
+                            float const ol = __shfl_down_sync(0xffffffffu, rl, off, S);
+                            combineComp(rh, rl, oh, ol);
+                        }
+                        rhoD = double(rh) + double(rl);
+                    }
+                    else
+                    {
+                        double v = rho.value();
+                        for(int off = S >> 1; off > 0; off >>= 1)
+                            v += __shfl_down_sync(0xffffffffu, v, off, S);
+                        rhoD = v;
+                    }
+                    if(!lead)
+                        continue;
                     c.cur.rho[t] = rhoD;
                     c.lists.count[t] = nl;
                     double Bv[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
@@ -387,8 +465,16 @@ namespace sph
         //! Physics variants compiled separately: 0 = the reference's inviscid
         //! hydro, 1 = hydro + viscosity, 2 = SPMHD (viscosity, Dedner and the
         //! tensile correction switched at run time).
+        //!
+        //! Accumulators (compensated in FP32): a (pressure, viscosity and magnetic
+        //! force together), D = sum m_j s_i v_ij.r (P dV work, div v and the
+        //! induction's B_i term), the viscous heating, T = sum m_j s_i (B_i.r) v_ij
+        //! + rho_i^2 (Dedner gradient term) for the induction, and the div B sum.
+        //! With the tensile correction the Maxwell-stress force and the Borve term
+        //! combine to sum m_j s_j (B_j.r)/(mu0 rho_j^2) (B_j - B_i).
+        //! The next neighbour's records are loaded before the current one is used.
         template<int K, typename T, int PH>
-        __global__ void __launch_bounds__(kForceThreads) kForce(DevCtx c, PhysArgs pa)
+        __global__ void __launch_bounds__(kForceThreads, sizeof(T) == 4 ? kForceMinBlocks : 3) kForce(DevCtx c, PhysArgs pa)
         {
             using V4 = typename PairCfg<T>::V4;
             Records<V4, T> const rec = records<T>(c);
@@ -405,23 +491,49 @@ namespace sph
                 V4 const pi = ld4(rec.pm + t);
                 V4 const vi = ld4(rec.fv + t);
                 V4 const ti = ld4(rec.ft + t);
-                V4 const bi = ld4(rec.fb + t);
+                V4 bi{};
+                if constexpr(PH == 2)
+                    bi = ld4(rec.fb + t);
                 HConst<T> const hk = hconst<K, T>(vi.w);
                 T const alpha = T(pa.alpha), beta = T(pa.beta), eps = T(pa.avEps);
-                Acc<T> ax, ay, az, D, duav, anx, any, anz, tens, t3x, t3y, t3z, divb, gpx, gpy, gpz;
+                T const rho2i = ti.x * ti.x;
+                Acc<T> ax, ay, az, D, duav, tx, ty, tz, divb;
                 T vsig = ti.z;
                 uint32_t const n = min(c.lists.count[t], c.lists.cap);
                 uint32_t const* row = c.lists.list + size_t(t) * c.lists.cap;
+                // software pipeline: records of entry k+1 are in flight while k is used
+                V4 npm{}, nfv{}, nft{}, nfb{};
+                uint32_t nslot = 0;
+                if(n > 0)
+                {
+                    uint32_t const e = row[0];
+                    uint32_t const j = e >> 5;
+                    nslot = e & 31u;
+                    npm = ld4(rec.pm + j);
+                    nfv = ld4(rec.fv + j);
+                    nft = ld4(rec.ft + j);
+                    if constexpr(PH == 2)
+                        nfb = ld4(rec.fb + j);
+                }
                 for(uint32_t k0 = 0; k0 < n; k0 += kBlock)
                 {
                     uint32_t const k1 = min(n, k0 + kBlock);
                     for(uint32_t k = k0; k < k1; ++k)
                     {
-                        uint32_t const e = row[k];
-                        uint32_t const j = e >> 5, sl = e & 31u;
-                        V4 const pj = ld4(rec.pm + j);
-                        V4 const vj = ld4(rec.fv + j);
-                        V4 const tj = ld4(rec.ft + j);
+                        V4 const pj = npm, vj = nfv, tj = nft;
+                        V4 const bj = nfb;
+                        uint32_t const sl = nslot;
+                        if(k + 1 < n)
+                        {
+                            uint32_t const e = row[k + 1];
+                            uint32_t const j = e >> 5;
+                            nslot = e & 31u;
+                            npm = ld4(rec.pm + j);
+                            nfv = ld4(rec.fv + j);
+                            nft = ld4(rec.ft + j);
+                            if constexpr(PH == 2)
+                                nfb = ld4(rec.fb + j);
+                        }
                         T const rx = pi.x - (pj.x + T(stencilOff(sl, 0)) * ex);
                         T const ry = pi.y - (pj.y + T(stencilOff(sl, 1)) * ey);
                         T const rz = pi.z - (pj.z + T(stencilOff(sl, 2)) * ez);
@@ -438,14 +550,9 @@ namespace sph
                         T const mj = pj.w;
                         T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
                         T const vr = vx * rx + vy * ry + vz * rz;
-                        // Isotropic pressure gradient (HydroForces.hpp:155-166).
-                        T const fiso = mj * (ti.y * si + tj.y * sj);
-                        ax.add(-fiso * rx);
-                        ay.add(-fiso * ry);
-                        az.add(-fiso * rz);
-                        // sum m_j s_i v_ij.r: P dV work, div v and the induction term.
                         T const msi = mj * si;
-                        D.add(msi * vr);
+                        // Isotropic pressure gradient (HydroForces.hpp:155-166).
+                        T f = -mj * (ti.y * si + tj.y * sj);
                         if(av && vr < T(0))
                         {
                             T const hb = T(0.5) * (vi.w + vj.w);
@@ -454,38 +561,51 @@ namespace sph
                             T const rb = T(0.5) * (ti.x + tj.x);
                             T const Pi = (-alpha * cb * mu + beta * mu * mu) / rb;
                             T const g = mj * Pi * T(0.5) * (si + sj);
-                            ax.add(-g * rx);
-                            ay.add(-g * ry);
-                            az.add(-g * rz);
+                            f -= g;
                             duav.add(T(0.5) * g * vr);
                         }
+                        T fx = f * rx, fy = f * ry, fz = f * rz;
+                        D.add(msi * vr);
                         T const w = vr * invR;
                         T const vs = ti.z + tj.z - beta * (w < T(0) ? w : T(0));
                         vsig = vs > vsig ? vs : vsig;
                         if constexpr(PH == 2)
                         {
-                            V4 const bj = ld4(rec.fb + j);
                             T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
                             T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
-                            T const ci = msi * Bir * ti.w;
                             T const cj = mj * sj * Bjr * tj.w;
-                            anx.add(ci * bi.x + cj * bj.x);
-                            any.add(ci * bi.y + cj * bj.y);
-                            anz.add(ci * bi.z + cj * bj.z);
-                            tens.add(ci + cj);
+                            if(tensile)
+                            {
+                                // stress + Borve: c_i B_i + c_j B_j - B_i (c_i + c_j) = c_j (B_j - B_i)
+                                fx += cj * (bj.x - bi.x);
+                                fy += cj * (bj.y - bi.y);
+                                fz += cj * (bj.z - bi.z);
+                            }
+                            else
+                            {
+                                T const ci = msi * Bir * ti.w;
+                                fx += ci * bi.x + cj * bj.x;
+                                fy += ci * bi.y + cj * bj.y;
+                                fz += ci * bi.z + cj * bj.z;
+                            }
                             T const wB = msi * Bir;
-                            t3x.add(wB * vx);
-                            t3y.add(wB * vy);
-                            t3z.add(wB * vz);
-                            divb.add(msi * (Bir - Bjr));
+                            T gx = wB * vx, gy = wB * vy, gz = wB * vz;
                             if(dedner)
                             {
-                                T const g = mj * (bi.w * si + bj.w * sj);
-                                gpx.add(g * rx);
-                                gpy.add(g * ry);
-                                gpz.add(g * rz);
+                                // rho_i^2 * m_j (psi_i/rho_i^2 s_i + psi_j/rho_j^2 s_j) r
+                                T const g = rho2i * mj * (bi.w * si + bj.w * sj);
+                                gx += g * rx;
+                                gy += g * ry;
+                                gz += g * rz;
                             }
+                            tx.add(gx);
+                            ty.add(gy);
+                            tz.add(gz);
+                            divb.add(msi * (Bir - Bjr));
                         }
+                        ax.add(fx);
+                        ay.add(fy);
+                        az.add(fz);
                     }
                     ax.fold();
                     ay.fold();
@@ -494,49 +614,32 @@ namespace sph
                     duav.fold();
                     if constexpr(PH == 2)
                     {
-                        anx.fold();
-                        any.fold();
-                        anz.fold();
-                        tens.fold();
-                        t3x.fold();
-                        t3y.fold();
-                        t3z.fold();
+                        tx.fold();
+                        ty.fold();
+                        tz.fold();
                         divb.fold();
-                        gpx.fold();
-                        gpy.fold();
-                        gpz.fold();
                     }
                 }
                 // Epilogue in FP64.
                 double const rho = c.cur.rho[t];
                 double const h = c.cur.h[t];
                 double const pr2 = (pa.gamma - 1.0) * c.cur.u[t] / rho; // P_i / rho_i^2
-                double a[3] = {ax.value(), ay.value(), az.value()};
+                double const a[3] = {ax.value(), ay.value(), az.value()};
                 double const Dv = D.value();
                 c.d.dudt[t] = pr2 * Dv + duav.value();
                 if constexpr(PH == 2)
                 {
                     double const Bi[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
                     double const psi = c.cur.psi[t];
-                    double const an[3] = {anx.value(), any.value(), anz.value()};
-                    double const tsum = tens.value();
-                    double const t3[3] = {t3x.value(), t3y.value(), t3z.value()};
-                    double const gp[3] = {gpx.value(), gpy.value(), gpz.value()};
+                    double const tv[3] = {tx.value(), ty.value(), tz.value()};
                     double const invRho = 1.0 / rho;
                     double const divB = -invRho * divb.value();
                     double const divv = -invRho * Dv;
                     double const ch = __longlong_as_double(static_cast<long long>(c.scal->chBits));
+                    // dB/dt = -(1/rho)(T_induction - B_i D) - rho grad(psi); T carries rho^2 grad(psi)/rho.
 #pragma unroll
                     for(int q = 0; q < 3; ++q)
-                    {
-                        a[q] += an[q];
-                        if(tensile)
-                            a[q] -= Bi[q] * tsum;
-                        double dB = -invRho * (t3[q] - Bi[q] * Dv);
-                        if(dedner)
-                            dB -= rho * gp[q];
-                        c.d.dBdt[q][t] = dB;
-                    }
+                        c.d.dBdt[q][t] = -invRho * (tv[q] - Bi[q] * Dv);
                     c.d.divB[t] = divB;
                     c.d.dpsidt[t] = dedner ? (-ch * ch * divB - psi * pa.sigma * ch / h - 0.5 * psi * divv) : 0.0;
                 }

@@ -217,7 +217,10 @@ namespace sph
     void launchFinalize(DevCtx const& c, bool cfl, cudaStream_t s);
     void launchUnpermute(uint32_t n, uint32_t const* id, double const* src, double* dst, cudaStream_t s);
     void launchUnpermuteInt(uint32_t n, uint32_t const* id, uint32_t const* src, int32_t* dst, cudaStream_t s);
-    void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, cudaStream_t s);
+    //! Per-box conserved sums into out[nbox][kDiagWords]; scratch holds
+    //! boxReduceScratchDoubles(nbox) doubles.
+    void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, double* scratch, cudaStream_t s);
+    size_t boxReduceScratchDoubles(uint32_t nbox);
     void launchFill(double* p, size_t n, double v, cudaStream_t s);
     void launchGatherSpecies(
         uint32_t n,

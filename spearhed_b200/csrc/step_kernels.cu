@@ -340,45 +340,80 @@ namespace sph
                 p[i] = v;
         }
 
-        //! Per-box conserved sums: one block per box over its cells' targets.
-        __global__ void __launch_bounds__(kThreads) kBoxReduce(DevCtx c, PhysArgs pa, double* out)
+        //! Sorted-particle range [first, last) of every box's sources: one block
+        //! per box takes the min start / max end over the box's non-empty cells.
+        __global__ void __launch_bounds__(kThreads) kBoxRange(DevCtx c, uint32_t* range)
+        {
+            __shared__ uint32_t lo[kThreads], hi[kThreads];
+            BoxDev const& B = c.boxes[blockIdx.x];
+            uint32_t l = 0xffffffffu, h = 0;
+            for(uint32_t lc = threadIdx.x; lc < B.ncells; lc += kThreads)
+            {
+                uint32_t const cell = B.cellBase + lc;
+                uint32_t const s = c.cells.start[cell], e = c.cells.end[cell];
+                if(e > s)
+                {
+                    l = min(l, s);
+                    h = max(h, e);
+                }
+            }
+            lo[threadIdx.x] = l;
+            hi[threadIdx.x] = h;
+            __syncthreads();
+            for(int k = kThreads / 2; k > 0; k >>= 1)
+            {
+                if(int(threadIdx.x) < k)
+                {
+                    lo[threadIdx.x] = min(lo[threadIdx.x], lo[threadIdx.x + k]);
+                    hi[threadIdx.x] = max(hi[threadIdx.x], hi[threadIdx.x + k]);
+                }
+                __syncthreads();
+            }
+            if(threadIdx.x == 0)
+            {
+                range[2 * blockIdx.x] = lo[0] == 0xffffffffu ? 0u : lo[0];
+                range[2 * blockIdx.x + 1] = hi[0];
+            }
+        }
+
+        //! Conserved-sum partials of box blockIdx.x, slice blockIdx.y of kBoxSlices:
+        //! each block strides over its box's sorted range in a fixed order.
+        __global__ void __launch_bounds__(kThreads)
+            kBoxPartials(DevCtx c, PhysArgs pa, uint32_t const* range, double* partials)
         {
             __shared__ double red[kThreads / 32][kDiagWords];
-            BoxDev const& B = c.boxes[blockIdx.x];
             bool const mhd = pa.physics & SPH_PHYS_MHD;
+            uint32_t const first = range[2 * blockIdx.x], last = range[2 * blockIdx.x + 1];
             double acc[kDiagWords];
 #pragma unroll
             for(int k = 0; k < kDiagWords; ++k)
                 acc[k] = 0.0;
-            for(uint32_t lc = 0; lc < B.ncells; ++lc)
+            for(uint32_t p = first + blockIdx.y * kThreads + threadIdx.x; p < last; p += gridDim.y * kThreads)
             {
-                uint32_t const cell = B.cellBase + lc;
-                uint32_t const s = c.cells.start[cell], e = c.cells.mid[cell];
-                for(uint32_t p = s + threadIdx.x; p < e; p += kThreads)
+                if(!isTarget(c.cur.role[p]))
+                    continue;
+                double const m = c.cur.m[p];
+                double v2 = 0.0, B2 = 0.0;
+                for(int a = 0; a < 3; ++a)
                 {
-                    double const m = c.cur.m[p];
-                    double v2 = 0.0, B2 = 0.0;
-                    for(int a = 0; a < 3; ++a)
-                    {
-                        double const va = c.cur.v[a][p];
-                        v2 += va * va;
-                        acc[3 + a] += m * va;
-                        if(mhd)
-                            B2 += c.cur.B[a][p] * c.cur.B[a][p];
-                    }
-                    acc[0] += 0.5 * m * v2;
-                    acc[1] += m * c.cur.u[p];
-                    if(mhd && c.cur.rho[p] > 0.0)
-                        acc[2] += 0.5 * m * B2 / (pa.mu0 * c.cur.rho[p]);
-                    if(mhd && B2 > 0.0)
-                    {
-                        double const e2 = fabs(c.d.divB[p]) * c.cur.h[p] / sqrt(B2);
-                        acc[6] += e2;
-                        acc[7] += 1.0;
-                        acc[8] = fmax(acc[8], e2);
-                    }
-                    acc[9] += 1.0;
+                    double const va = c.cur.v[a][p];
+                    v2 += va * va;
+                    acc[3 + a] += m * va;
+                    if(mhd)
+                        B2 += c.cur.B[a][p] * c.cur.B[a][p];
                 }
+                acc[0] += 0.5 * m * v2;
+                acc[1] += m * c.cur.u[p];
+                if(mhd && c.cur.rho[p] > 0.0)
+                    acc[2] += 0.5 * m * B2 / (pa.mu0 * c.cur.rho[p]);
+                if(mhd && B2 > 0.0)
+                {
+                    double const e2 = fabs(c.d.divB[p]) * c.cur.h[p] / sqrt(B2);
+                    acc[6] += e2;
+                    acc[7] += 1.0;
+                    acc[8] = fmax(acc[8], e2);
+                }
+                acc[9] += 1.0;
             }
             int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -395,7 +430,25 @@ namespace sph
                 double r = 0.0;
                 for(int w = 0; w < kThreads / 32; ++w)
                     r = (k == 8) ? fmax(r, red[w][k]) : r + red[w][k];
-                out[size_t(blockIdx.x) * kDiagWords + k] = r;
+                partials[(size_t(blockIdx.x) * gridDim.y + blockIdx.y) * kDiagWords + k] = r;
+            }
+        }
+
+        //! Per box: the slices' partials summed in slice order.
+        __global__ void kBoxFinal(uint32_t nbox, uint32_t slices, double const* partials, double* out)
+        {
+            uint32_t const b = blockIdx.x * blockDim.x + threadIdx.x;
+            if(b >= nbox)
+                return;
+            for(int k = 0; k < kDiagWords; ++k)
+            {
+                double r = 0.0;
+                for(uint32_t sl = 0; sl < slices; ++sl)
+                {
+                    double const v = partials[(size_t(b) * slices + sl) * kDiagWords + k];
+                    r = (k == 8) ? fmax(r, v) : r + v;
+                }
+                out[size_t(b) * kDiagWords + k] = r;
             }
         }
     } // namespace
@@ -476,10 +529,24 @@ namespace sph
         }
     }
 
-    void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, cudaStream_t s)
+    void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, double* scratch, cudaStream_t s)
     {
-        kBoxReduce<<<c.nbox, kThreads, 0, s>>>(c, pa, out);
+        // scratch: 2*nbox range words (as doubles' storage) + nbox*slices*kDiagWords partials
+        uint32_t const slices = c.nbox == 1 ? 256u : (c.nbox < 64 ? 16u : 2u);
+        uint32_t* range = reinterpret_cast<uint32_t*>(scratch);
+        double* partials = scratch + c.nbox;
+        kBoxRange<<<c.nbox, kThreads, 0, s>>>(c, range);
         countLaunches(1);
+        kBoxPartials<<<dim3(c.nbox, slices), kThreads, 0, s>>>(c, pa, range, partials);
+        countLaunches(1);
+        kBoxFinal<<<(c.nbox + 127) / 128, 128, 0, s>>>(c.nbox, slices, partials, out);
+        countLaunches(1);
+    }
+
+    size_t boxReduceScratchDoubles(uint32_t nbox)
+    {
+        uint32_t const slices = nbox == 1 ? 256u : (nbox < 64 ? 16u : 2u);
+        return size_t(nbox) + size_t(nbox) * slices * kDiagWords;
     }
 
     void launchGatherSpecies(
