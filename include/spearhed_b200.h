@@ -60,7 +60,8 @@ enum
     SPH_PHYS_MHD = 1u << 1,      /* SPMHD induction + Maxwell stress                         */
     SPH_PHYS_DEDNER = 1u << 2,   /* Dedner/Tricco-Price hyperbolic divergence cleaning       */
     SPH_PHYS_TENSILE = 1u << 3,  /* Borve tensile-instability correction of the stress       */
-    SPH_PHYS_CFL = 1u << 4       /* adaptive dt from the CFL/force criteria (FP64 min)       */
+    SPH_PHYS_CFL = 1u << 4,      /* adaptive dt from the CFL/force criteria (FP64 min)       */
+    SPH_PHYS_ADAPTIVE_H = 1u << 5 /* h = hfact (m/rho)^(1/3) after every kick (needs SPH_CULL_PAIR_MAX) */
 };
 
 /* ---- precision of the pair kernels -------------------------------------- */
@@ -117,6 +118,9 @@ typedef struct SphParams
     double mu0;            /* magnetic permeability in code units (1)                        */
     int32_t max_neighbours;/* per-particle neighbour-list capacity; 0 = library default      */
     int32_t device;        /* CUDA device ordinal                                           */
+    double hfact;          /* eta of SPH_PHYS_ADAPTIVE_H: h = hfact * (m/rho)^(1/3), e.g. 1.2 */
+    double h_max;          /* largest h the run may reach: sets the cell size and caps adaptive h;
+                              0 = the largest input h (times 1.5 with SPH_PHYS_ADAPTIVE_H)    */
 } SphParams;
 
 /* A particle box: the reference's fluid/wall domain (an AABB, spmacc/particles/regions/AABB.hpp:38-127).
@@ -230,6 +234,12 @@ int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts);
  * in milliseconds: [0] sort+permute, [1] density, [2] force, [3] integrate+reduce,
  * [4] whole call.  n is the array length (<= 5). */
 int sph_get_timings(sph_ctx* ctx, int32_t n, double* ms);
+
+/* Per-box simulated time and the dt the next step will use (nbox entries each):
+ * the clock a checkpoint must save and restore.  No reference counterpart (the
+ * reference's checkpointing is disabled, include/spearhed/control/Simulation.hpp:54-61). */
+int sph_get_clock(sph_ctx* ctx, int32_t nbox, double* time, double* dt_next);
+int sph_set_clock(sph_ctx* ctx, int32_t nbox, const double* time, const double* dt_next);
 
 /* Capture each later sph_step's per-step launch sequence in a CUDA graph and
  * replay it (on = 1) or launch the kernels one by one (on = 0, the default). */

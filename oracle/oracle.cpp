@@ -273,6 +273,7 @@ namespace orc
         std::vector<int64_t> cellOf; // global cell id, -1 for non-sources
         std::vector<int64_t> cellStart; // CSR over global cells (sources only)
         std::vector<int64_t> cellItems;
+        std::vector<double> hcap;
         int64_t ncellTotal = 0;
 
         bool isTarget(int64_t i) const
@@ -306,10 +307,27 @@ namespace orc
             }
         }
         s.grids.resize(s.nbox);
+        s.hcap.assign(s.nbox, 0.0);
         int64_t base = 0;
         for(int b = 0; b < s.nbox; ++b)
         {
-            int const st = makeGrid(s.boxes[b], cellRadius(sup, hmax[b]), s.grids[b]);
+            // Same rule as the CUDA path: h_max when given, else the largest h
+            // (x1.5 under adaptive h); the oracle re-derives it every step, so
+            // adaptive-h parity runs pass h_max explicitly.
+            double hgrid = hmax[b];
+            if(s.p.cull == SPH_CULL_PAIR_MAX)
+            {
+                if(s.p.h_max > 0.0)
+                {
+                    if(s.p.h_max < hmax[b])
+                        return SPH_ERR_INVALID;
+                    hgrid = s.p.h_max;
+                }
+                else if(s.p.physics & SPH_PHYS_ADAPTIVE_H)
+                    hgrid = 1.5 * hmax[b];
+            }
+            s.hcap[b] = hgrid;
+            int const st = makeGrid(s.boxes[b], cellRadius(sup, hgrid), s.grids[b]);
             if(st != SPH_OK)
                 return st;
             s.grids[b].base = base;
@@ -513,10 +531,11 @@ namespace orc
         return d;
     }
 
+    //! Per box: the Dedner speed used and the CFL minimum; accepted pairs in total.
     struct ForceOut
     {
-        double ch = 0.0;
-        double dtmin = 0.0;
+        std::vector<double> ch;
+        std::vector<double> dtmin;
         double pairs = 0.0;
     };
 
@@ -530,18 +549,20 @@ namespace orc
         bool const tensile = mhd && (p.physics & SPH_PHYS_TENSILE);
         double const mu0 = p.mu0 > 0 ? p.mu0 : 1.0;
         std::vector<Derived> der(s.n);
-        double ch = 0.0;
+        // each box of an ensemble has its own cleaning speed and CFL minimum
+        std::vector<double> chBox(s.nbox, 0.0);
         for(int64_t i = 0; i < s.n; ++i)
             if(s.isSource(i) || s.isTarget(i))
             {
                 der[i] = derived(s, i);
                 if(s.isTarget(i))
-                    ch = std::max(ch, der[i].c);
+                    chBox[s.boxOf[i]] = std::max(chBox[s.boxOf[i]], der[i].c);
             }
-        double dtmin = 1e300;
+        std::vector<double> dtBox(s.nbox, 1e300);
         double pairs = 0.0;
-#pragma omp parallel reduction(min : dtmin) reduction(+ : pairs)
+#pragma omp parallel reduction(+ : pairs)
         {
+            std::vector<double> dtLocal(s.nbox, 1e300);
             std::vector<Pair> nb;
 #pragma omp for schedule(dynamic, 256)
             for(int64_t i = 0; i < s.n; ++i)
@@ -554,6 +575,7 @@ namespace orc
                     neighbours<double>(s, i, nb);
                 pairs += double(nb.size());
                 Derived const& di = der[i];
+                double const ch = chBox[s.boxOf[i]];
                 double const hi = col(s.v->h, i, p.h0);
                 double const vi[3] = {col(s.v->vel[0], i), col(s.v->vel[1], i), col(s.v->vel[2], i)};
                 double const Bi[3] = {col(s.v->B[0], i), col(s.v->B[1], i), col(s.v->B[2], i)};
@@ -664,12 +686,15 @@ namespace orc
                 double const amag = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
                 if(amag > 0.0 && p.cfl_force > 0.0)
                     dt = std::min(dt, p.cfl_force * std::sqrt(hi / amag));
-                dtmin = std::min(dtmin, dt);
+                dtLocal[s.boxOf[i]] = std::min(dtLocal[s.boxOf[i]], dt);
             }
+#pragma omp critical
+            for(int b = 0; b < s.nbox; ++b)
+                dtBox[b] = std::min(dtBox[b], dtLocal[b]);
         }
         ForceOut fo;
-        fo.ch = ch;
-        fo.dtmin = dtmin;
+        fo.ch = chBox;
+        fo.dtmin = dtBox;
         fo.pairs = pairs;
         return fo;
     }
@@ -1009,10 +1034,13 @@ extern "C"
         orc::ForceOut fo = orc::withKernel(
             s.p.kernel,
             [&](auto k) { return orc::forcePass<decltype(k)>(s, geom_fp32 != 0); });
-        if(ch)
-            *ch = fo.ch;
-        if(dtmin)
-            *dtmin = fo.dtmin;
+        for(int b = 0; b < nbox; ++b)
+        {
+            if(ch)
+                ch[b] = fo.ch[b];
+            if(dtmin)
+                dtmin[b] = fo.dtmin[b];
+        }
         return SPH_OK;
     }
 
@@ -1041,8 +1069,8 @@ extern "C"
 
     /** Simulation::runOneStep, n_steps times (Simulation.x.cpp:233-300):
      *  drift (Movable), density, forces, kick (Movable & Thermodynamic).
-     *  dt_state holds the dt of the next step (updated from the CFL criterion when
-     *  SPH_PHYS_CFL is set); time accumulates simulated time. */
+     *  dt_state[b] holds box b's dt of the next step (updated from the box's CFL
+     *  minimum when SPH_PHYS_CFL is set); time[b] accumulates its simulated time. */
     int orc_step(
         SphParams const* p,
         int32_t nbox,
@@ -1058,15 +1086,18 @@ extern "C"
     {
         if(!p || !dt_state || !time)
             return SPH_ERR_INVALID;
+        std::vector<double> dtUsed(nbox);
         for(int32_t step = 0; step < n_steps; ++step)
         {
-            double const dt = *dt_state;
+            for(int b = 0; b < nbox; ++b)
+                dtUsed[b] = dt_state[b];
             // drift: r += v dt (PushVelocity.hpp:38-41); periodic wrap into [lo, hi)
             for(int64_t i = 0; i < n; ++i)
             {
                 if(!(roles[i] & SPH_ROLE_MOVABLE))
                     continue;
                 int const b = v->box_id ? v->box_id[i] : 0;
+                double const dt = dtUsed[b];
                 for(int a = 0; a < 3; ++a)
                 {
                     double x = v->pos[a][i] + orc::col(v->vel[a], i) * dt;
@@ -1101,9 +1132,17 @@ extern "C"
             {
                 if(!s.isTarget(i))
                     continue;
+                double const dt = dtUsed[s.boxOf[i]];
                 for(int a = 0; a < 3; ++a)
                     v->vel[a][i] += v->dvdt[a][i] * dt;
                 v->u[i] += v->dudt[i] * dt;
+                if((p->physics & SPH_PHYS_ADAPTIVE_H) && v->h)
+                {
+                    // h for the next step: hfact (m/rho)^(1/3), capped by the cell size
+                    double const hn = p->hfact * std::cbrt(v->mass[i] / v->density[i]);
+                    double const cap = s.hcap[s.boxOf[i]];
+                    v->h[i] = hn < cap ? hn : cap;
+                }
                 if(mhd)
                 {
                     for(int a = 0; a < 3; ++a)
@@ -1112,16 +1151,19 @@ extern "C"
                         v->psi[i] += v->dpsidt[i] * dt;
                 }
             }
-            *time += dt;
-            if(p->physics & SPH_PHYS_CFL)
-                *dt_state = fo.dtmin;
+            for(int b = 0; b < nbox; ++b)
+            {
+                time[b] += dtUsed[b];
+                if((p->physics & SPH_PHYS_CFL) && fo.dtmin[b] < 1e300)
+                    dt_state[b] = fo.dtmin[b];
+            }
             if(diag)
             {
                 orc::diagnostics(s, *diag);
-                diag->time = *time;
-                diag->dt = dt;
-                diag->dt_next = *dt_state;
-                diag->c_h = fo.ch;
+                diag->time = time[0];
+                diag->dt = dtUsed[0];
+                diag->dt_next = dt_state[0];
+                diag->c_h = fo.ch[0];
                 diag->pairs = fo.pairs;
                 diag->steps = step + 1;
             }

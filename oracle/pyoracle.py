@@ -173,10 +173,13 @@ class System:
         _check(orc().orc_density(*self._common(), int(fp32_geometry)))
 
     def force(self, fp32_geometry=False):
-        ch = C.c_double(0)
-        dtm = C.c_double(0)
-        _check(orc().orc_force(*self._common(), int(fp32_geometry), C.byref(ch), C.byref(dtm)))
-        return ch.value, dtm.value
+        """Runs the force pass; returns (c_h, CFL minimum) — per box for an ensemble."""
+        ch = np.zeros(self.nbox)
+        dtm = np.zeros(self.nbox)
+        _check(orc().orc_force(*self._common(), int(fp32_geometry), _ptr(ch, C.c_double), _ptr(dtm, C.c_double)))
+        if self.nbox == 1:
+            return float(ch[0]), float(dtm[0])
+        return ch, dtm
 
     def reduce(self):
         d = SphDiag()
@@ -184,12 +187,15 @@ class System:
         return d
 
     def step(self, n_steps, dt_state, time=0.0, fp32_geometry=False):
-        dts = C.c_double(dt_state)
-        t = C.c_double(time)
+        """n_steps of the full step; dt_state and time are per box (scalars for one box)."""
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt_state, dtype=np.float64), (self.nbox,)))
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (self.nbox,)))
         d = SphDiag()
-        _check(orc().orc_step(*self._common(), int(fp32_geometry), int(n_steps), C.byref(dts), C.byref(t),
-                              C.byref(d)))
-        return dts.value, t.value, d
+        _check(orc().orc_step(*self._common(), int(fp32_geometry), int(n_steps), _ptr(dts, C.c_double),
+                              _ptr(t, C.c_double), C.byref(d)))
+        if self.nbox == 1:
+            return float(dts[0]), float(t[0]), d
+        return dts, t, d
 
 
 def _check(st):

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import abi
 from .abi import (  # noqa: F401  (re-exported names)
-    CULL_GLOBAL, CULL_PAIR_MAX, KERNEL_CUBIC, KERNEL_QUINTIC, KERNEL_WENDLAND_C2, PHYS_AV, PHYS_CFL,
+    CULL_GLOBAL, CULL_PAIR_MAX, KERNEL_CUBIC, KERNEL_QUINTIC, KERNEL_WENDLAND_C2, PHYS_ADAPTIVE_H, PHYS_AV, PHYS_CFL,
     PHYS_DEDNER, PHYS_MHD, PHYS_TENSILE, PREC_FP32_COMP, PREC_FP64, ROLES_BOUNDARY, ROLES_DEFAULT,
     ROLES_TRACER, SPECIES_BOUNDARY, SPECIES_DEFAULT, SPECIES_ROLES, SPECIES_TRACER, SphBox, SphDiag,
     SphError, SphParams, Species, default_params, make_box,
@@ -91,6 +91,22 @@ class Context:
         ms = (C.c_double * 5)()
         abi.check(self._L.sph_get_timings(self._p, 5, ms))
         return list(ms)
+
+    def clock(self):
+        """(time, dt_next) per box."""
+        n = max(self.nbox, 1)
+        t = np.zeros(n)
+        d = np.zeros(n)
+        P = C.POINTER(C.c_double)
+        abi.check(self._L.sph_get_clock(self._p, n, t.ctypes.data_as(P), d.ctypes.data_as(P)))
+        return t, d
+
+    def set_clock(self, time, dt_next):
+        n = max(self.nbox, 1)
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (n,)))
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt_next, dtype=np.float64), (n,)))
+        P = C.POINTER(C.c_double)
+        abi.check(self._L.sph_set_clock(self._p, n, t.ctypes.data_as(P), d.ctypes.data_as(P)))
 
     def use_graph(self, on: bool = True):
         abi.check(self._L.sph_use_graph(self._p, int(bool(on))))

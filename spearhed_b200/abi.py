@@ -27,7 +27,7 @@ SPH_ERR_TIMEOUT = 8
 SPH_ERR_UNSUPPORTED = 9
 
 KERNEL_CUBIC, KERNEL_QUINTIC, KERNEL_WENDLAND_C2 = 0, 1, 2
-PHYS_AV, PHYS_MHD, PHYS_DEDNER, PHYS_TENSILE, PHYS_CFL = 1, 2, 4, 8, 16
+PHYS_AV, PHYS_MHD, PHYS_DEDNER, PHYS_TENSILE, PHYS_CFL, PHYS_ADAPTIVE_H = 1, 2, 4, 8, 16, 32
 PREC_FP64, PREC_FP32_COMP = 0, 1
 CULL_GLOBAL, CULL_PAIR_MAX = 0, 1
 SPECIES_DEFAULT, SPECIES_BOUNDARY, SPECIES_TRACER = 0, 1, 2
@@ -59,6 +59,8 @@ class SphParams(C.Structure):
         ("mu0", C.c_double),
         ("max_neighbours", C.c_int32),
         ("device", C.c_int32),
+        ("hfact", C.c_double),
+        ("h_max", C.c_double),
     ]
 
 
@@ -114,7 +116,7 @@ def default_params(**kw) -> SphParams:
     p = SphParams(
         kernel=KERNEL_CUBIC, precision=PREC_FP32_COMP, cull=CULL_GLOBAL, physics=0,
         gamma=5.0 / 3.0, h0=0.05, dt=0.01, alpha=1.0, beta=2.0, av_eps=0.01, cfl=0.3,
-        cfl_force=0.25, dedner_sigma=1.0, mu0=1.0, max_neighbours=0, device=0,
+        cfl_force=0.25, dedner_sigma=1.0, mu0=1.0, max_neighbours=0, device=0, hfact=1.2, h_max=0.0,
     )
     for k, v in kw.items():
         setattr(p, k, v)
@@ -211,6 +213,8 @@ def lib():
         "sph_get_neighbour_counts": (C.c_int, [ctx_p, C.c_int32, P(C.c_int32)]),
         "sph_get_timings": (C.c_int, [ctx_p, C.c_int32, P(C.c_double)]),
         "sph_use_graph": (C.c_int, [ctx_p, C.c_int32]),
+        "sph_get_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
+        "sph_set_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_last_error_string": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

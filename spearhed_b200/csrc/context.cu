@@ -134,6 +134,10 @@ namespace
             return fail(SPH_ERR_INVALID, "Dedner cleaning needs SPH_PHYS_MHD");
         if(p.max_neighbours < 0)
             return fail(SPH_ERR_INVALID, "max_neighbours must be >= 0");
+        if((p.physics & SPH_PHYS_ADAPTIVE_H) && (p.cull != SPH_CULL_PAIR_MAX || !(p.hfact > 0.0)))
+            return fail(SPH_ERR_INVALID, "adaptive h needs SPH_CULL_PAIR_MAX and hfact > 0");
+        if(p.h_max < 0.0 || !std::isfinite(p.h_max))
+            return fail(SPH_ERR_INVALID, "h_max must be >= 0");
         return SPH_OK;
     }
 } // namespace
@@ -302,6 +306,7 @@ struct sph_ctx
         pa.cflForce = p.cfl_force;
         pa.sigma = p.dedner_sigma;
         pa.h0 = p.h0;
+        pa.hfact = p.hfact;
         pa.physics = p.physics;
         pa.cull = p.cull;
     }
@@ -412,7 +417,21 @@ int sph_ctx::layout()
     for(int32_t b = 0; b < nbox; ++b)
     {
         SphBox const& B = boxes[b];
-        double const rc = cellRadius(sup, hmax[b]);
+        // The cell size admits h up to hgrid: h_max when given, else the largest
+        // input h (with 50% room to grow under adaptive h).
+        double hgrid = hmax[b];
+        if(p.cull == SPH_CULL_PAIR_MAX)
+        {
+            if(p.h_max > 0.0)
+            {
+                if(p.h_max < hmax[b])
+                    return fail(SPH_ERR_INVALID, "an input h exceeds params.h_max");
+                hgrid = p.h_max;
+            }
+            else if(p.physics & SPH_PHYS_ADAPTIVE_H)
+                hgrid = 1.5 * hmax[b];
+        }
+        double const rc = cellRadius(sup, hgrid);
         sph::BoxDev& d = boxDesc[b];
         uint64_t cells = 1;
         for(int a = 0; a < 3; ++a)
@@ -432,6 +451,7 @@ int sph_ctx::layout()
         }
         d.cellBase = uint32_t(cellBase);
         d.ncells = uint32_t(cells);
+        d.hcap = hgrid;
         cellBase += cells;
         if(cellBase * 2 + 1 >= (1ull << 32))
             return fail(SPH_ERR_UNSUPPORTED, "too many cells (2^31)");
@@ -475,6 +495,9 @@ int sph_ctx::allocate()
        || (st = alloc(dc.sortScratch, sph::radixScratchWords(n))))
         return st;
     if((st = alloc(dc.status, sph::kStatWords)) || (st = alloc(dc.scal, 1)) || (st = alloc(dc.diag, sph::kDiagWords)))
+        return st;
+    if((st = alloc(dc.bs.dt, nbox)) || (st = alloc(dc.bs.time, nbox)) || (st = alloc(dc.bs.lastDt, nbox))
+       || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)))
         return st;
     dc.nPartialBlocks = sph::partialBlocks(n);
     if((st = alloc(dc.partials, size_t(dc.nPartialBlocks) * sph::kDiagWords))
@@ -528,8 +551,12 @@ int sph_ctx::uploadMirror()
         cudaMemcpyHostToDevice,
         stream));
     sph::StepScalars sc{};
-    sc.dt = p.dt;
     SPH_CUDA_TRY(cudaMemcpyAsync(dc.scal, &sc, sizeof(sc), cudaMemcpyHostToDevice, stream));
+    std::vector<double> dts(boxDesc.size(), p.dt);
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.bs.dt, dts.data(), 8 * dts.size(), cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.time, 0, 8 * dts.size(), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.lastDt, 0, 8 * dts.size(), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, 8 * dts.size(), stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
     mirrorStale = false;
     deviceCurrent = true;
@@ -637,7 +664,7 @@ int sph_ctx::build(bool drift)
 {
     SPH_CUDA_TRY(cudaMemsetAsync(dc.status, 0, sizeof(uint32_t) * sph::kStatWords, stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
-    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->chBits, 0, sizeof(unsigned long long), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, sizeof(unsigned long long) * dc.nbox, stream));
     sph::launchDriftKeys(dc, drift, stream);
     bool const inB = sph::radixSortPairs(dc.keysA, dc.valsA, dc.keysB, dc.valsB, n, dc.keyBits, dc.sortScratch, stream);
     uint32_t const* keys = inB ? dc.keysB : dc.keysA;
@@ -658,7 +685,7 @@ int sph_ctx::densityPass()
 
 int sph_ctx::forcePass()
 {
-    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->dtBits, 0x7f, sizeof(unsigned long long), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.dtBits, 0x7f, sizeof(unsigned long long) * dc.nbox, stream));
     sph::launchForce(dc, pa, p.kernel, p.precision, stream);
     return SPH_OK;
 }
@@ -716,7 +743,7 @@ int sph_ctx::steps(int32_t nsteps, double dt)
     if(st)
         return st;
     if(dt > 0.0)
-        SPH_CUDA_TRY(cudaMemcpyAsync(&dc.scal->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, stream));
+        sph::launchFill(dc.bs.dt, dc.nbox, dt, stream);
     for(double& t : timings)
         t = 0.0;
     bool const graph = useGraph && nsteps >= 2;
@@ -791,24 +818,15 @@ int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
     int st = stagingCols(kHostCols);
     if(st)
         return st;
-    for(int c = 0; c < kHostCols; ++c)
-    {
-        double const* src = viewCol(v, c);
-        if(c == cH && src)
-            for(int64_t i = 0; i < s.n; ++i)
-                if(!(src[i] > 0.0) || !std::isfinite(src[i]))
-                    return fail(SPH_ERR_NONFINITE, "smoothing length must be positive and finite");
-        if(c == cM && src && (s.roles & SPH_ROLE_SOURCE))
-            for(int64_t i = 0; i < s.n; ++i)
-                if(!(src[i] > 0.0))
-                    return fail(SPH_ERR_NONFINITE, "source particle mass must be positive");
-    }
+    // h and source masses are checked on the device as they are gathered
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.status + sph::kStatBadInput, 0, sizeof(uint32_t), stream));
     for(int c = 0; c < kHostCols; ++c)
     {
         double const* src = viewCol(v, c);
         double* stage = staging[c];
         if(src)
             SPH_CUDA_TRY(cudaMemcpyAsync(stage + s.offset, src, size_t(s.n) * 8, cudaMemcpyHostToDevice, stream));
+        bool const mustBePositive = c == cH || (c == cM && (s.roles & SPH_ROLE_SOURCE));
         sph::launchGatherSpecies(
             n,
             dc.cur.id,
@@ -817,6 +835,7 @@ int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
             src ? stage : nullptr,
             colDefault(c),
             masterCol(dc.cur, c),
+            mustBePositive ? dc.status + sph::kStatBadInput : nullptr,
             stream);
     }
     if(v && v->box_id)
@@ -829,8 +848,16 @@ int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
         SPH_CUDA_TRY(cudaMemcpyAsync(stage + s.offset, v->box_id, size_t(s.n) * 4, cudaMemcpyHostToDevice, stream));
         sph::launchGatherSpeciesInt(n, dc.cur.id, s.offset, uint32_t(s.n), stage, dc.cur.box, stream);
     }
+    uint32_t bad = 0;
+    SPH_CUDA_TRY(cudaMemcpyAsync(&bad, dc.status + sph::kStatBadInput, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
     mirrorStale = true;
+    if(bad)
+        return fail(
+            SPH_ERR_NONFINITE,
+            std::to_string(bad)
+                + " smoothing lengths or source masses are not positive and finite; the species holds them until it "
+                  "is set again");
     densityValid = false;
     forceValid = false;
     return SPH_OK;
@@ -967,7 +994,7 @@ int sph_density(sph_ctx* ctx)
             return st;
         SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.status, 0, sizeof(uint32_t) * sph::kStatWords, ctx->stream));
         SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->pairs, 0, sizeof(unsigned long long), ctx->stream));
-        SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->chBits, 0, sizeof(unsigned long long), ctx->stream));
+        SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.bs.chBits, 0, sizeof(unsigned long long) * ctx->dc.nbox, ctx->stream));
         if((st = ctx->densityPass()) || (st = ctx->checkStatus("sph_density")))
             return st;
     }
@@ -1094,21 +1121,36 @@ int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts)
 
 namespace
 {
-    int reduceBoxes(sph_ctx* ctx, std::vector<double>& perBox, sph::StepScalars& sc, double* diag)
+    //! Per-box step state copied back to the host.
+    struct HostBoxState
+    {
+        std::vector<double> dt, time, lastDt;
+        std::vector<unsigned long long> ch;
+    };
+
+    int reduceBoxes(sph_ctx* ctx, std::vector<double>& perBox, sph::StepScalars& sc, HostBoxState& hb)
     {
         int st = ctx->ensureDevice();
         if(st)
             return st;
+        uint32_t const nbox = ctx->dc.nbox;
         sph::launchBoxReduce(ctx->dc, ctx->pa, ctx->boxOut, ctx->boxScratch, ctx->stream);
-        perBox.resize(size_t(ctx->dc.nbox) * sph::kDiagWords);
+        perBox.resize(size_t(nbox) * sph::kDiagWords);
+        hb.dt.resize(nbox);
+        hb.time.resize(nbox);
+        hb.lastDt.resize(nbox);
+        hb.ch.resize(nbox);
         SPH_CUDA_TRY(cudaMemcpyAsync(perBox.data(), ctx->boxOut, perBox.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
         SPH_CUDA_TRY(cudaMemcpyAsync(&sc, ctx->dc.scal, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
-        SPH_CUDA_TRY(cudaMemcpyAsync(diag, ctx->dc.diag, sizeof(double) * sph::kDiagWords, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(hb.dt.data(), ctx->dc.bs.dt, 8 * nbox, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(hb.time.data(), ctx->dc.bs.time, 8 * nbox, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(hb.lastDt.data(), ctx->dc.bs.lastDt, 8 * nbox, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(hb.ch.data(), ctx->dc.bs.chBits, 8 * nbox, cudaMemcpyDeviceToHost, ctx->stream));
         SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         return SPH_OK;
     }
 
-    void fillDiag(SphDiag& o, double const* a, sph::StepScalars const& sc, double const* diag)
+    void fillDiag(SphDiag& o, double const* a, sph::StepScalars const& sc, HostBoxState const& hb, uint32_t b)
     {
         o.e_kin = a[0];
         o.e_int = a[1];
@@ -1119,10 +1161,10 @@ namespace
         o.divb_mean = a[7] > 0 ? a[6] / a[7] : 0.0;
         o.divb_max = a[8];
         o.n_targets = int64_t(a[9]);
-        o.time = sc.time;
-        o.dt = diag[10];
-        o.dt_next = sc.dt;
-        o.c_h = __builtin_bit_cast(double, sc.chBits);
+        o.time = hb.time[b];
+        o.dt = hb.lastDt[b];
+        o.dt_next = hb.dt[b];
+        o.c_h = __builtin_bit_cast(double, hb.ch[b]);
         o.pairs = double(sc.pairs);
         o.steps = sc.steps;
         o.pairs_total = sc.pairsAccum;
@@ -1136,8 +1178,8 @@ int sph_reduce(sph_ctx* ctx, SphDiag* out)
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     std::vector<double> pb;
     sph::StepScalars sc{};
-    double diag[sph::kDiagWords] = {};
-    int st = reduceBoxes(ctx, pb, sc, diag);
+    HostBoxState hb;
+    int st = reduceBoxes(ctx, pb, sc, hb);
     if(st)
         return st;
     double a[sph::kDiagWords] = {};
@@ -1148,7 +1190,13 @@ int sph_reduce(sph_ctx* ctx, SphDiag* out)
             a[k] = (k == 8) ? std::max(a[k], v) : a[k] + v;
         }
     *out = SphDiag{};
-    fillDiag(*out, a, sc, diag);
+    fillDiag(*out, a, sc, hb, 0);
+    // an ensemble reports the largest c_h and the smallest next dt over its boxes
+    for(uint32_t b = 1; b < ctx->dc.nbox; ++b)
+    {
+        out->c_h = std::max(out->c_h, __builtin_bit_cast(double, hb.ch[b]));
+        out->dt_next = std::min(out->dt_next, hb.dt[b]);
+    }
     return SPH_OK;
 }
 
@@ -1159,8 +1207,8 @@ int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     std::vector<double> pb;
     sph::StepScalars sc{};
-    double diag[sph::kDiagWords] = {};
-    int st = reduceBoxes(ctx, pb, sc, diag);
+    HostBoxState hb;
+    int st = reduceBoxes(ctx, pb, sc, hb);
     if(st)
         return st;
     if(uint32_t(nbox) != ctx->dc.nbox)
@@ -1168,8 +1216,43 @@ int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
     for(int32_t b = 0; b < nbox; ++b)
     {
         out[b] = SphDiag{};
-        fillDiag(out[b], &pb[size_t(b) * sph::kDiagWords], sc, diag);
+        fillDiag(out[b], &pb[size_t(b) * sph::kDiagWords], sc, hb, uint32_t(b));
     }
+    return SPH_OK;
+}
+
+int sph_get_clock(sph_ctx* ctx, int32_t nbox, double* time, double* dt_next)
+{
+    if(!ctx || nbox < 1 || !time || !dt_next)
+        return fail(SPH_ERR_INVALID, "sph_get_clock: bad arguments");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->ensureDevice();
+    if(st)
+        return st;
+    if(uint32_t(nbox) != ctx->dc.nbox)
+        return fail(SPH_ERR_INVALID, "sph_get_clock: nbox differs from the context's box count");
+    SPH_CUDA_TRY(cudaMemcpyAsync(time, ctx->dc.bs.time, 8 * size_t(nbox), cudaMemcpyDeviceToHost, ctx->stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(dt_next, ctx->dc.bs.dt, 8 * size_t(nbox), cudaMemcpyDeviceToHost, ctx->stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_set_clock(sph_ctx* ctx, int32_t nbox, double const* time, double const* dt_next)
+{
+    if(!ctx || nbox < 1 || !time || !dt_next)
+        return fail(SPH_ERR_INVALID, "sph_set_clock: bad arguments");
+    for(int32_t b = 0; b < nbox; ++b)
+        if(!std::isfinite(time[b]) || !(dt_next[b] > 0.0) || !std::isfinite(dt_next[b]))
+            return fail(SPH_ERR_INVALID, "sph_set_clock: time must be finite and dt positive");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int st = ctx->ensureDevice();
+    if(st)
+        return st;
+    if(uint32_t(nbox) != ctx->dc.nbox)
+        return fail(SPH_ERR_INVALID, "sph_set_clock: nbox differs from the context's box count");
+    SPH_CUDA_TRY(cudaMemcpyAsync(ctx->dc.bs.time, time, 8 * size_t(nbox), cudaMemcpyHostToDevice, ctx->stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(ctx->dc.bs.dt, dt_next, 8 * size_t(nbox), cudaMemcpyHostToDevice, ctx->stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return SPH_OK;
 }
 

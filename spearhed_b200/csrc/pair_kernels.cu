@@ -98,11 +98,22 @@ namespace sph
         }
         __device__ __forceinline__ float rcpT(float x)
         {
-            return __frcp_rn(x);
+            return __fdividef(1.0f, x);
         }
         __device__ __forceinline__ double rcpT(double x)
         {
             return 1.0 / x;
+        }
+
+        //! Division in the pair precision: fast in FP32 (the pair terms carry no
+        //! tighter requirement), IEEE in FP64.
+        __device__ __forceinline__ float divT(float a, float b)
+        {
+            return __fdividef(a, b);
+        }
+        __device__ __forceinline__ double divT(double a, double b)
+        {
+            return a / b;
         }
 
         template<typename T>
@@ -203,12 +214,243 @@ namespace sph
             lo = lo + olo + e;
         }
 
+        //! Per-lane state of one chunk of up to 32 targets of a cell.
+        template<typename V4, typename T>
+        struct TargetChunk
+        {
+            V4 own;
+            T hi;
+            uint32_t t;        //!< sorted target index
+            uint32_t nl;       //!< accepted so far (same on every lane of the target's group)
+            uint32_t groupBase, groupMask, subBelow;
+            int S, sub;
+            bool act;
+        };
+
+        template<typename V4, typename T>
+        __device__ __forceinline__ void initChunk(
+            TargetChunk<V4, T>& ch,
+            Records<V4, T> const& rec,
+            uint32_t tc,
+            uint32_t tEnd,
+            int lane)
+        {
+            uint32_t const nt = tc < tEnd ? min(32u, tEnd - tc) : 0u;
+            ch.S = subLanes(nt == 0 ? 32u : nt);
+            ch.sub = lane & (ch.S - 1);
+            uint32_t const tt = uint32_t(lane) / uint32_t(ch.S);
+            ch.groupBase = tt * uint32_t(ch.S);
+            ch.groupMask = ch.S == 32 ? 0xffffffffu : (((1u << ch.S) - 1u) << ch.groupBase);
+            ch.subBelow = (1u << ch.sub) - 1u;
+            ch.act = tt < nt;
+            ch.t = tc + tt;
+            ch.nl = 0;
+            ch.own = V4{};
+            ch.hi = T(1);
+            if(ch.act)
+            {
+                ch.own = ld4(rec.pm + ch.t);
+                ch.hi = rec.hc[ch.t];
+            }
+        }
+
+        //! Cull the staged candidates [0, m) against one target chunk and append
+        //! the accepted entries, in candidate order, to each target's list row.
+        template<typename V4, typename T, bool PAIRMAX>
+        __device__ __forceinline__ void cullChunk(
+            TargetChunk<V4, T>& ch,
+            V4 const* sPos,
+            T const* sH,
+            uint32_t const* sEnt,
+            uint32_t m,
+            T supT,
+            T R2g,
+            uint32_t* list,
+            uint32_t cap,
+            bool countOnly)
+        {
+            constexpr int U = 4;
+            uint32_t* const row = list + size_t(ch.t) * cap;
+            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
+            if(ch.S == 1)
+            {
+                // Full chunk: every lane its own target, all lanes read the same
+                // candidate (shared-memory broadcast); bounds are warp-uniform.
+                uint32_t q0 = 0;
+                for(; q0 + U <= m; q0 += U)
+                {
+                    bool acc[U];
+                    uint32_t ent[U];
+#pragma unroll
+                    for(int u = 0; u < U; ++u)
+                    {
+                        V4 const pj = sPos[q0 + u];
+                        T const dx = subRn(ch.own.x, pj.x);
+                        T const dy = subRn(ch.own.y, pj.y);
+                        T const dz = subRn(ch.own.z, pj.z);
+                        T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
+                        T R2 = R2g;
+                        if constexpr(PAIRMAX)
+                        {
+                            T const hj = sH[q0 + u];
+                            T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
+                            R2 = mulRn(R, R);
+                        }
+                        ent[u] = sEnt[q0 + u];
+                        acc[u] = r2 < R2;
+                    }
+#pragma unroll
+                    for(int u = 0; u < U; ++u)
+                        if(acc[u] && ch.act && ent[u] != selfEnt)
+                        {
+                            if(!countOnly && ch.nl < cap)
+                                row[ch.nl] = ent[u];
+                            ++ch.nl;
+                        }
+                }
+                for(; q0 < m; ++q0)
+                {
+                    V4 const pj = sPos[q0];
+                    T const dx = subRn(ch.own.x, pj.x);
+                    T const dy = subRn(ch.own.y, pj.y);
+                    T const dz = subRn(ch.own.z, pj.z);
+                    T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
+                    T R2 = R2g;
+                    if constexpr(PAIRMAX)
+                    {
+                        T const hj = sH[q0];
+                        T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
+                        R2 = mulRn(R, R);
+                    }
+                    uint32_t const e = sEnt[q0];
+                    if(r2 < R2 && ch.act && e != selfEnt)
+                    {
+                        if(!countOnly && ch.nl < cap)
+                            row[ch.nl] = e;
+                        ++ch.nl;
+                    }
+                }
+                return;
+            }
+            // Short chunk: S lanes per target test interleaved candidates
+            // q = q0 + u*S + sub; ballots keep the candidate order.
+            int const S = ch.S;
+            for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(U * S))
+            {
+                bool accU[U];
+                uint32_t entU[U];
+#pragma unroll
+                for(int u = 0; u < U; ++u)
+                {
+                    uint32_t const q = q0 + uint32_t(u * S + ch.sub);
+                    bool const ok = ch.act && q < m;
+                    uint32_t const qq = ok ? q : 0u;
+                    V4 const pj = sPos[qq];
+                    T const dx = subRn(ch.own.x, pj.x);
+                    T const dy = subRn(ch.own.y, pj.y);
+                    T const dz = subRn(ch.own.z, pj.z);
+                    T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
+                    T R2 = R2g;
+                    if constexpr(PAIRMAX)
+                    {
+                        T const hj = sH[qq];
+                        T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
+                        R2 = mulRn(R, R);
+                    }
+                    entU[u] = sEnt[qq];
+                    accU[u] = ok && r2 < R2 && entU[u] != selfEnt;
+                }
+#pragma unroll
+                for(int u = 0; u < U; ++u)
+                {
+                    uint32_t const bits = __ballot_sync(0xffffffffu, accU[u]) & ch.groupMask;
+                    if(accU[u])
+                    {
+                        uint32_t const k = ch.nl + __popc((bits >> ch.groupBase) & ch.subBelow);
+                        if(!countOnly && k < cap)
+                            row[k] = entU[u];
+                    }
+                    ch.nl += __popc(bits);
+                }
+            }
+        }
+
+        //! Density of one target chunk over its list rows; writes rho, the
+        //! count and the force-pass records.  Returns the chunk's max c.
+        template<int K, typename V4, typename T>
+        __device__ __forceinline__ double densityChunk(
+            TargetChunk<V4, T> const& ch,
+            DevCtx const& c,
+            Records<V4, T> const& rec,
+            PhysArgs const& pa,
+            T ex,
+            T ey,
+            T ez,
+            uint32_t cap)
+        {
+            bool const lead = ch.act && ch.sub == 0;
+            uint32_t const n = ch.act ? min(ch.nl, cap) : 0u;
+            uint32_t const* row = c.lists.list + size_t(ch.t) * cap;
+            HConst<T> const hk = hconst<K, T>(ch.hi);
+            Acc<T> rho;
+            if(lead)
+                rho.add(ch.own.w * kernelW<K, T>(T(0), hk));
+            int const S = ch.S;
+            uint32_t k = uint32_t(ch.sub);
+            while(k < n)
+            {
+                for(int b = 0; b < kBlock && k < n; ++b, k += uint32_t(S))
+                {
+                    uint32_t const e = row[k];
+                    uint32_t const j = e >> 5, sl = e & 31u;
+                    V4 const pj = ld4(rec.pm + j);
+                    T const dx = ch.own.x - (pj.x + T(stencilOff(sl, 0)) * ex);
+                    T const dy = ch.own.y - (pj.y + T(stencilOff(sl, 1)) * ey);
+                    T const dz = ch.own.z - (pj.z + T(stencilOff(sl, 2)) * ez);
+                    T const r2 = dx * dx + dy * dy + dz * dz;
+                    T const r = r2 > T(0) ? r2 * rsqrtT(r2) : T(0);
+                    rho.add(pj.w * kernelW<K, T>(r, hk));
+                }
+                rho.fold();
+            }
+            rho.fold();
+            double rhoD;
+            if constexpr(sizeof(T) == 4)
+            {
+                float rh = rho.c.hi, rl = rho.c.lo;
+                for(int off = S >> 1; off > 0; off >>= 1)
+                {
+                    float const oh = __shfl_down_sync(0xffffffffu, rh, off, S);
+                    float const ol = __shfl_down_sync(0xffffffffu, rl, off, S);
+                    combineComp(rh, rl, oh, ol);
+                }
+                rhoD = double(rh) + double(rl);
+            }
+            else
+            {
+                double v = rho.value();
+                for(int off = S >> 1; off > 0; off >>= 1)
+                    v += __shfl_down_sync(0xffffffffu, v, off, S);
+                rhoD = v;
+            }
+            if(!lead)
+                return 0.0;
+            uint32_t const t = ch.t;
+            c.cur.rho[t] = rhoD;
+            c.lists.count[t] = ch.nl;
+            double Bv[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
+            double ft[4], fb[4];
+            derivedRecord(rhoD, c.cur.u[t], Bv, c.cur.psi[t], pa, ft, fb);
+            rec.ft[t] = mk4<V4>(ft[0], ft[1], ft[2], ft[3]);
+            rec.fb[t] = mk4<V4>(fb[0], fb[1], fb[2], fb[3]);
+            return ft[2];
+        }
+
         template<int K, typename T, bool PAIRMAX>
-        __global__ void __launch_bounds__(kDensWarps * 32) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
+        __global__ void __launch_bounds__(kDensWarps * 32, sizeof(T) == 4 ? 6 : 4) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
         {
             using V4 = typename PairCfg<T>::V4;
             constexpr int CAP = PairCfg<T>::cap;
-            constexpr int U = 4; //!< candidates per lane per cull iteration (independent chains)
             extern __shared__ __align__(32) unsigned char smem[];
             int const warp = threadIdx.x >> 5;
             int const lane = threadIdx.x & 31;
@@ -225,6 +467,7 @@ namespace sph
             uint32_t maxCount = 0;
             unsigned long long pairs = 0;
             double chMax = 0.0;
+            int chBox = -1; // box whose c_h maximum chMax holds (warp-uniform)
 
             for(uint32_t cell = blockIdx.x * kDensWarps + warp; cell < c.cells.ncells; cell += nWarps)
             {
@@ -232,7 +475,17 @@ namespace sph
                 uint32_t const tEnd = c.cells.mid[cell];
                 if(tBeg >= tEnd)
                     continue;
-                BoxDev const& B = c.boxes[boxOfCell(c.boxes, c.nbox, cell)];
+                int const box = boxOfCell(c.boxes, c.nbox, cell);
+                if(box != chBox)
+                {
+                    // flush the previous box's signal-speed maximum
+                    double const m = warpMaxD(chMax);
+                    if(lane == 0 && chBox >= 0 && !countOnly)
+                        atomicMax(&c.bs.chBits[chBox], orderedBits(m));
+                    chMax = 0.0;
+                    chBox = box;
+                }
+                BoxDev const& B = c.boxes[box];
                 uint32_t const lc = cell - B.cellBase;
                 int const cc[3]
                     = {int(lc % uint32_t(B.n[0])), int((lc / uint32_t(B.n[0])) % uint32_t(B.n[1])),
@@ -279,27 +532,13 @@ namespace sph
                 uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
                 T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
 
-                for(uint32_t tc = tBeg; tc < tEnd; tc += 32)
+                // Two target chunks (up to 64 targets) share every staged window.
+                for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
                 {
-                    uint32_t const nt = min(32u, tEnd - tc);
-                    int const S = subLanes(nt);
-                    int const sub = lane & (S - 1);
-                    uint32_t const tt = uint32_t(lane) / uint32_t(S);
-                    uint32_t const groupBase = tt * uint32_t(S);
-                    uint32_t const groupMask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << groupBase);
-                    uint32_t const subBelow = (1u << sub) - 1u;
-                    bool const act = tt < nt;
-                    uint32_t const t = tc + tt;
-                    V4 own{};
-                    T hi = T(1);
-                    if(act)
-                    {
-                        own = ld4(rec.pm + t);
-                        hi = rec.hc[t];
-                    }
-                    uint32_t const selfEnt = packEntry(t, kCentreSlot);
-                    uint32_t* row = c.lists.list + size_t(t) * cap;
-                    uint32_t nl = 0; // same value on every lane of the target's group
+                    TargetChunk<V4, T> A, Bc;
+                    initChunk(A, rec, tc, tEnd, lane);
+                    bool const twoChunks = tc + 32 < tEnd;
+                    initChunk(Bc, rec, tc + 32, tEnd, lane);
                     for(uint32_t cb = 0; cb < total; cb += CAP)
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
@@ -308,6 +547,8 @@ namespace sph
                         {
                             uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
                             uint32_t const n0 = __shfl_sync(0xffffffffu, sCnt, sl);
+                            if(p0 + n0 <= cb || p0 >= ce)
+                                continue; // uniform: slot outside this window
                             uint32_t const b0 = __shfl_sync(0xffffffffu, sBeg, sl);
                             T const sx = __shfl_sync(0xffffffffu, sh[0], sl);
                             T const sy = __shfl_sync(0xffffffffu, sh[1], sl);
@@ -329,123 +570,19 @@ namespace sph
                         }
                         __syncwarp();
                         uint32_t const m = ce - cb;
-                        // The warp walks candidates in order; lane (tt, sub) tests
-                        // candidates q = q0 + u*S + sub.  Accepted entries keep the
-                        // candidate order in the row.
-                        for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(U * S))
-                        {
-                            bool accU[U];
-                            uint32_t entU[U];
-#pragma unroll
-                            for(int u = 0; u < U; ++u)
-                            {
-                                uint32_t const q = q0 + uint32_t(u * S + sub);
-                                bool ok = act && q < m;
-                                uint32_t const qq = ok ? q : 0u;
-                                V4 const pj = sPos[qq];
-                                T const dx = subRn(own.x, pj.x);
-                                T const dy = subRn(own.y, pj.y);
-                                T const dz = subRn(own.z, pj.z);
-                                T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
-                                T R2 = R2g;
-                                if constexpr(PAIRMAX)
-                                {
-                                    T const hj = sH[qq];
-                                    T const R = mulRn(supT, hi > hj ? hi : hj);
-                                    R2 = mulRn(R, R);
-                                }
-                                entU[u] = sEnt[qq];
-                                accU[u] = ok && r2 < R2 && entU[u] != selfEnt;
-                            }
-                            if(S == 1)
-                            {
-#pragma unroll
-                                for(int u = 0; u < U; ++u)
-                                    if(accU[u])
-                                    {
-                                        if(!countOnly && nl < cap)
-                                            row[nl] = entU[u];
-                                        ++nl;
-                                    }
-                            }
-                            else
-                            {
-#pragma unroll
-                                for(int u = 0; u < U; ++u)
-                                {
-                                    uint32_t const bits = __ballot_sync(0xffffffffu, accU[u]) & groupMask;
-                                    if(accU[u])
-                                    {
-                                        uint32_t const k = nl + __popc((bits >> groupBase) & subBelow);
-                                        if(!countOnly && k < cap)
-                                            row[k] = entU[u];
-                                    }
-                                    nl += __popc(bits);
-                                }
-                            }
-                        }
+                        cullChunk<V4, T, PAIRMAX>(A, sPos, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                        if(twoChunks)
+                            cullChunk<V4, T, PAIRMAX>(Bc, sPos, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
                     }
-                    bool const lead = act && sub == 0;
-                    maxCount = max(maxCount, lead ? nl : 0u);
-                    pairs += lead ? nl : 0u;
+                    bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
+                    maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
+                    pairs += (leadA ? A.nl : 0u) + (leadB ? Bc.nl : 0u);
                     if(countOnly)
                         continue;
                     __syncwarp();
-                    // Density over the compact row (DensitySummation.hpp:57-93):
-                    // rho_i = m_i W(0, h_i) + sum_j m_j W(r_ij, h_i); the S lanes of a
-                    // target take every S-th entry and their partials are combined.
-                    uint32_t const n = act ? min(nl, cap) : 0u;
-                    HConst<T> const hk = hconst<K, T>(hi);
-                    Acc<T> rho;
-                    if(lead)
-                        rho.add(own.w * kernelW<K, T>(T(0), hk));
-                    uint32_t k = uint32_t(sub);
-                    while(k < n)
-                    {
-                        for(int b = 0; b < kBlock && k < n; ++b, k += uint32_t(S))
-                        {
-                            uint32_t const e = row[k];
-                            uint32_t const j = e >> 5, sl = e & 31u;
-                            V4 const pj = ld4(rec.pm + j);
-                            T const dx = own.x - (pj.x + T(stencilOff(sl, 0)) * ex);
-                            T const dy = own.y - (pj.y + T(stencilOff(sl, 1)) * ey);
-                            T const dz = own.z - (pj.z + T(stencilOff(sl, 2)) * ez);
-                            T const r2 = dx * dx + dy * dy + dz * dz;
-                            T const r = r2 > T(0) ? r2 * rsqrtT(r2) : T(0);
-                            rho.add(pj.w * kernelW<K, T>(r, hk));
-                        }
-                        rho.fold();
-                    }
-                    rho.fold();
-                    double rhoD;
-                    if constexpr(sizeof(T) == 4)
-                    {
-                        float rh = rho.c.hi, rl = rho.c.lo;
-                        for(int off = S >> 1; off > 0; off >>= 1)
-                        {
-                            float const oh = __shfl_down_sync(0xffffffffu, rh, off, S);
-                            float const ol = __shfl_down_sync(0xffffffffu, rl, off, S);
-                            combineComp(rh, rl, oh, ol);
-                        }
-                        rhoD = double(rh) + double(rl);
-                    }
-                    else
-                    {
-                        double v = rho.value();
-                        for(int off = S >> 1; off > 0; off >>= 1)
-                            v += __shfl_down_sync(0xffffffffu, v, off, S);
-                        rhoD = v;
-                    }
-                    if(!lead)
-                        continue;
-                    c.cur.rho[t] = rhoD;
-                    c.lists.count[t] = nl;
-                    double Bv[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
-                    double ft[4], fb[4];
-                    derivedRecord(rhoD, c.cur.u[t], Bv, c.cur.psi[t], pa, ft, fb);
-                    rec.ft[t] = mk4<V4>(ft[0], ft[1], ft[2], ft[3]);
-                    rec.fb[t] = mk4<V4>(fb[0], fb[1], fb[2], fb[3]);
-                    chMax = fmax(chMax, ft[2]);
+                    chMax = fmax(chMax, densityChunk<K>(A, c, rec, pa, ex, ey, ez, cap));
+                    if(twoChunks)
+                        chMax = fmax(chMax, densityChunk<K>(Bc, c, rec, pa, ex, ey, ez, cap));
                 }
             }
             maxCount = warpMaxU(maxCount);
@@ -457,8 +594,8 @@ namespace sph
                     atomicMax(&c.status[kStatOverflow], maxCount);
                 atomicMax(&c.status[kStatMaxCount], maxCount);
                 atomicAdd(&c.scal->pairs, pairs);
-                if(!countOnly)
-                    atomicMax(&c.scal->chBits, orderedBits(chMax));
+                if(!countOnly && chBox >= 0)
+                    atomicMax(&c.bs.chBits[chBox], orderedBits(chMax));
             }
         }
 
@@ -481,6 +618,7 @@ namespace sph
             uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
             bool const act = t < c.n && isTarget(c.cur.role[t]);
             double dtLocal = 1e300;
+            int const myBox = t < c.n ? c.cur.box[t] : -1;
             if(act)
             {
                 bool const av = (PH == 1) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
@@ -556,10 +694,10 @@ namespace sph
                         if(av && vr < T(0))
                         {
                             T const hb = T(0.5) * (vi.w + vj.w);
-                            T const mu = hb * vr / (r2 + eps * hb * hb);
+                            T const mu = divT(hb * vr, r2 + eps * hb * hb);
                             T const cb = T(0.5) * (ti.z + tj.z);
                             T const rb = T(0.5) * (ti.x + tj.x);
-                            T const Pi = (-alpha * cb * mu + beta * mu * mu) / rb;
+                            T const Pi = divT(-alpha * cb * mu + beta * mu * mu, rb);
                             T const g = mj * Pi * T(0.5) * (si + sj);
                             f -= g;
                             duav.add(T(0.5) * g * vr);
@@ -635,7 +773,7 @@ namespace sph
                     double const invRho = 1.0 / rho;
                     double const divB = -invRho * divb.value();
                     double const divv = -invRho * Dv;
-                    double const ch = __longlong_as_double(static_cast<long long>(c.scal->chBits));
+                    double const ch = __longlong_as_double(static_cast<long long>(c.bs.chBits[myBox]));
                     // dB/dt = -(1/rho)(T_induction - B_i D) - rho grad(psi); T carries rho^2 grad(psi)/rho.
 #pragma unroll
                     for(int q = 0; q < 3; ++q)
@@ -652,9 +790,16 @@ namespace sph
                     dt = fmin(dt, pa.cflForce * sqrt(h / amag));
                 dtLocal = dt;
             }
-            dtLocal = warpMinD(dtLocal);
-            if((threadIdx.x & 31) == 0 && dtLocal < 1e300)
-                atomicMin(&c.scal->dtBits, orderedBits(dtLocal));
+            // CFL minimum per box: one atomic per warp when the warp is in one box
+            int const box0 = __shfl_sync(0xffffffffu, myBox, 0);
+            if(__all_sync(0xffffffffu, myBox == box0 || dtLocal >= 1e300))
+            {
+                dtLocal = warpMinD(dtLocal);
+                if((threadIdx.x & 31) == 0 && dtLocal < 1e300)
+                    atomicMin(&c.bs.dtBits[box0], orderedBits(dtLocal));
+            }
+            else if(dtLocal < 1e300)
+                atomicMin(&c.bs.dtBits[myBox], orderedBits(dtLocal));
         }
 
         template<typename T>

@@ -23,6 +23,7 @@ namespace sph
         int32_t periodic[3];
         uint32_t cellBase; //!< first global cell id of this box
         uint32_t ncells;
+        double hcap; //!< largest h the cell size admits (adaptive h is capped here)
     };
 
     //! Roles (include/spearhed_b200.h, SPH_ROLE_*).
@@ -260,6 +261,7 @@ namespace sph
         kStatOutside = 1,    //!< particles found outside a non-periodic box
         kStatNonFinite = 2,  //!< non-finite positions
         kStatMaxCount = 3,   //!< largest neighbour count seen (list sizing)
+        kStatBadInput = 4,   //!< gathered h / source masses that are not positive and finite
         kStatWords = 8
     };
 } // namespace sph

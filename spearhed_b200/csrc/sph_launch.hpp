@@ -59,7 +59,7 @@ namespace sph
     //! Physics constants the kernels need (one copy per launch, by value).
     struct PhysArgs
     {
-        double gamma, alpha, beta, avEps, mu0, cfl, cflForce, sigma, h0;
+        double gamma, alpha, beta, avEps, mu0, cfl, cflForce, sigma, h0, hfact;
         uint32_t physics;
         int32_t cull;
     };
@@ -154,14 +154,21 @@ namespace sph
     //! Scalars the step keeps on the device so a step never waits for the host.
     struct StepScalars
     {
-        double dt;                 //!< dt of the current step
-        double time;               //!< simulated time
-        unsigned long long chBits; //!< max signal speed of the targets (Dedner c_h), ordered bits
-        unsigned long long dtBits; //!< min CFL dt over targets, ordered bits
         unsigned long long pairs;  //!< accepted ordered pairs of the last neighbour build
-        double chLast;             //!< c_h used by the last force pass
         double pairsAccum;         //!< accepted pairs summed over the steps taken
         long long steps;
+    };
+
+    //! Per-box step state (structure of arrays, nbox entries each).  Boxes of an
+    //! ensemble are independent: each has its own dt, time, CFL minimum and
+    //! Dedner cleaning speed.
+    struct BoxScalars
+    {
+        double* dt;                  //!< dt of the current step
+        double* time;                //!< simulated time
+        double* lastDt;              //!< dt of the last completed step
+        unsigned long long* dtBits;  //!< min CFL dt over the box's targets (ordered bits)
+        unsigned long long* chBits;  //!< max signal speed of the box's targets (ordered bits)
     };
 
     struct DevCtx
@@ -182,6 +189,7 @@ namespace sph
         uint32_t* sortScratch;
         uint32_t* status; //!< kStatWords words
         StepScalars* scal;
+        BoxScalars bs;
         double* partials; //!< per-block diagnostics partial sums
         double* diag;     //!< finalized diagnostics (kDiagWords)
         uint32_t nPartialBlocks;
@@ -222,6 +230,8 @@ namespace sph
     void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, double* scratch, cudaStream_t s);
     size_t boxReduceScratchDoubles(uint32_t nbox);
     void launchFill(double* p, size_t n, double v, cudaStream_t s);
+    //! master[p] = src[id[p]] for one species; badCount (or null) counts values
+    //! that are not positive and finite.
     void launchGatherSpecies(
         uint32_t n,
         uint32_t const* id,
@@ -230,6 +240,7 @@ namespace sph
         double const* src,
         double dflt,
         double* master,
+        uint32_t* badCount,
         cudaStream_t s);
     void launchGatherSpeciesInt(
         uint32_t n,

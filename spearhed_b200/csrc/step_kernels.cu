@@ -25,8 +25,9 @@ namespace sph
             if(p >= c.n)
                 return;
             uint8_t const role = c.cur.role[p];
-            BoxDev const& B = c.boxes[c.cur.box[p]];
-            double const dt = c.scal->dt;
+            int32_t const bx = c.cur.box[p];
+            BoxDev const& B = c.boxes[bx];
+            double const dt = c.bs.dt[bx];
             double x[3];
             bool finite = true;
 #pragma unroll
@@ -184,7 +185,7 @@ namespace sph
             bool const mhd = pa.physics & SPH_PHYS_MHD;
             if(p < c.n && isTarget(c.cur.role[p]))
             {
-                double const dt = c.scal->dt;
+                double const dt = c.bs.dt[c.cur.box[p]];
                 double const m = c.cur.m[p];
                 double v2 = 0.0, B2 = 0.0;
 #pragma unroll
@@ -211,6 +212,13 @@ namespace sph
                 acc[0] = 0.5 * m * v2;
                 acc[1] = m * u;
                 double const rho = c.cur.rho[p];
+                if(pa.physics & SPH_PHYS_ADAPTIVE_H)
+                {
+                    // h for the next step from this step's density, capped by the cell size
+                    double const hn = pa.hfact * cbrt(m / rho);
+                    double const cap = c.boxes[c.cur.box[p]].hcap;
+                    c.cur.h[p] = hn < cap ? hn : cap;
+                }
                 acc[2] = (mhd && rho > 0.0) ? 0.5 * m * B2 / (pa.mu0 * rho) : 0.0;
                 if(mhd && B2 > 0.0)
                 {
@@ -270,20 +278,25 @@ namespace sph
             if(threadIdx.x == 0)
             {
                 StepScalars& S = *c.scal;
-                double const dt = S.dt;
-                S.time += dt;
                 S.steps += 1;
                 S.pairsAccum += double(S.pairs);
 #pragma unroll
                 for(int k = 0; k < 10; ++k)
                     c.diag[k] = red[0][k];
-                c.diag[10] = dt;
-                c.diag[11] = S.time;
+                c.diag[10] = c.bs.dt[0];
+                c.diag[11] = c.bs.time[0] + c.bs.dt[0];
+            }
+            // every box advances by its own dt; with CFL its next dt is its own minimum
+            for(uint32_t b = threadIdx.x; b < c.nbox; b += kThreads)
+            {
+                double const dt = c.bs.dt[b];
+                c.bs.time[b] += dt;
+                c.bs.lastDt[b] = dt;
                 if(cfl)
                 {
-                    double const dtn = __longlong_as_double(static_cast<long long>(S.dtBits));
+                    double const dtn = __longlong_as_double(static_cast<long long>(c.bs.dtBits[b]));
                     if(dtn > 0.0 && dtn < 1e300)
-                        S.dt = dtn;
+                        c.bs.dt[b] = dtn;
                 }
             }
         }
@@ -309,14 +322,21 @@ namespace sph
             uint32_t cnt,
             double const* __restrict__ src,
             double dflt,
-            double* __restrict__ master)
+            double* __restrict__ master,
+            uint32_t* __restrict__ badCount)
         {
             uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
             if(p >= n)
                 return;
             uint32_t const i = id[p];
             if(i - off < cnt)
-                master[p] = src ? src[i] : dflt;
+            {
+                double const v = src ? src[i] : dflt;
+                // columns that must be positive and finite (h, source masses) pass a counter
+                if(badCount && !(v > 0.0 && isfinite(v)))
+                    atomicAdd(badCount, 1u);
+                master[p] = v;
+            }
         }
         __global__ void kGatherSpeciesInt(
             uint32_t n,
@@ -557,11 +577,13 @@ namespace sph
         double const* src,
         double dflt,
         double* master,
+        uint32_t* badCount,
         cudaStream_t s)
     {
         if(n)
         {
-            kGatherSpecies<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, dflt, master);
+            kGatherSpecies<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+                n, id, off, cnt, src, dflt, master, badCount);
             countLaunches(1);
         }
     }

@@ -67,7 +67,7 @@ def philox_uniform(seed, shape):
     return np.random.Generator(np.random.Philox(key=seed)).uniform(-1.0, 1.0, size=shape)
 
 
-def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False):
+def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False, hfact=1.2):
     """3D Sod shock tube, gamma 1.4, periodic in y and z.
 
     Left x in [-0.5, 0): rho 1, P 1 on a (64 s)x(16 s)x(16 s) lattice; right
@@ -89,15 +89,15 @@ def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False):
     s = abi.Species(n)
     s.pos[:] = np.concatenate([left, right], axis=1)
     s.mass[:] = m
-    s.h[:] = np.concatenate([np.full(left.shape[1], 1.2 * dxl), np.full(right.shape[1], 1.2 * dxr)])
+    s.h[:] = np.concatenate([np.full(left.shape[1], hfact * dxl), np.full(right.shape[1], hfact * dxr)])
     rho = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.125)])
     P = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.1)])
     s.density[:] = rho
     s.u[:] = P / ((gamma - 1.0) * rho)
-    physics = 0 if reference_physics else (abi.PHYS_AV | abi.PHYS_CFL)
+    physics = 0 if reference_physics else (abi.PHYS_AV | abi.PHYS_CFL | abi.PHYS_ADAPTIVE_H)
     params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
-                                physics=physics, gamma=gamma, h0=1.2 * dxr, dt=1e-4, alpha=1.0, beta=2.0,
-                                cfl=0.3)
+                                physics=physics, gamma=gamma, h0=hfact * dxr, dt=1e-4, alpha=1.0, beta=2.0,
+                                cfl=0.3, hfact=hfact, h_max=1.5 * hfact * dxr)
     box = abi.make_box((-0.75, 0.0, 0.0), (0.75, Ly, Ly), (0, 1, 1))
     return Workload("sod_small", params, [box], {abi.SPECIES_DEFAULT: s}, steps=50,
                     meta={"n_left": left.shape[1], "n_right": right.shape[1], "dx_left": dxl, "dx_right": dxr})
@@ -145,3 +145,67 @@ def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, jitter=0
     box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (1, 1, 1))
     return Workload("orszag_tang", params, [box], {abi.SPECIES_DEFAULT: s}, steps=200,
                     meta={"nx": nx, "nz": nz, "dx": dx})
+
+
+def brio_wu_box(n_target=8192, precision=abi.PREC_FP32_COMP, nt=8, box_id=0):
+    """One 3D Brio-Wu MHD shock tube (gamma 2, Bx 0.75).
+
+    Left x in [-0.5, 0): rho 1, P 1, By +1; right x in [0, 0.5): rho 0.125, P 0.1,
+    By -1.  Equal masses: the right lattice spacing is twice the left.  The tube
+    is nt left lattice layers thick in y and z (periodic); its length is chosen
+    so the box holds about n_target particles.  x is open (the box extends 0.25
+    beyond each end).  Cubic spline, AV, SPMHD with Dedner cleaning and the
+    tensile correction, adaptive h (hfact 1.2), CFL 0.3.
+    """
+    gamma = 2.0
+    nxl = max(8, int(round(n_target / (nt * nt * 1.125))))
+    nxl += nxl % 2
+    dxl = 0.5 / nxl
+    L = nt * dxl
+    left = lattice((-0.5, 0.0, 0.0), (0.0, L, L), (nxl, nt, nt))
+    right = lattice((0.0, 0.0, 0.0), (0.5, L, L), (nxl // 2, nt // 2, nt // 2))
+    n = left.shape[1] + right.shape[1]
+    s = abi.Species(n)
+    s.pos[:] = np.concatenate([left, right], axis=1)
+    m = dxl ** 3
+    s.mass[:] = m
+    isl = np.concatenate([np.ones(left.shape[1], bool), np.zeros(right.shape[1], bool)])
+    rho = np.where(isl, 1.0, 0.125)
+    P = np.where(isl, 1.0, 0.1)
+    s.density[:] = rho
+    s.u[:] = P / ((gamma - 1.0) * rho)
+    s.h[:] = np.where(isl, 1.2 * dxl, 2.4 * dxl)
+    s.B[0] = 0.75
+    s.B[1] = np.where(isl, 1.0, -1.0)
+    s.box_id[:] = box_id
+    physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
+               | abi.PHYS_ADAPTIVE_H)
+    params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                physics=physics, gamma=gamma, h0=2.4 * dxl, dt=1e-5, alpha=1.0, beta=2.0,
+                                cfl=0.3, hfact=1.2, h_max=3.6 * dxl)
+    box = abi.make_box((-0.75, 0.0, 0.0), (0.75, L, L), (0, 1, 1))
+    return params, box, s
+
+
+def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144):
+    """An ensemble of independent Brio-Wu tubes with particle counts drawn
+    log-uniform in [n_lo, n_hi] (numpy Philox, key ``seed``).  With the default
+    512 boxes this is about 31 M particles.  Every box keeps its own time step.
+    The ensemble-wide h_max is the largest box's (it sets no cell size: each box
+    has its own grid from its own h)."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    sizes = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=nbox)).astype(int)
+    boxes, parts, params = [], [], None
+    hmax = 0.0
+    for b, nb in enumerate(sizes):
+        p, box, s = brio_wu_box(int(nb), precision=precision, box_id=b)
+        boxes.append(box)
+        parts.append(s)
+        hmax = max(hmax, p.h_max)
+        params = p
+    species = abi.Species.concat(parts)
+    # boxes differ in resolution; h_max = 0 lets each box size its grid from its own
+    # largest h (x1.5 under adaptive h)
+    params.h_max = 0.0
+    return Workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: species}, steps=100,
+                    meta={"sizes": sizes.tolist(), "seed": seed})
