@@ -57,7 +57,34 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=5)
     ap.add_argument("--graph", action="store_true", help="replay the step as a CUDA graph")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="orszag_tang",
+                    choices=["orszag_tang", "kelvin_helmholtz", "mhd_rotor", "brio_wu_ensemble", "sod_small"],
+                    help="orszag_tang (the headline) or one of the other configurations")
+    ap.add_argument("--fp64-boxes", type=int, default=8,
+                    help="ensemble only: boxes of the FP64 single-box loop sample")
     return ap.parse_args()
+
+
+WORKLOADS = {
+    "orszag_tang": ("orszag_tang_slab_512x512x4", "wendland_c2", "mhd"),
+    "kelvin_helmholtz": ("kelvin_helmholtz_cube_16.8M", "wendland_c2", "mhd"),
+    "mhd_rotor": ("mhd_rotor_slab_1024x1024x4", "wendland_c2", "mhd"),
+    "brio_wu_ensemble": ("brio_wu_ensemble_512_boxes", "cubic", "mhd"),
+    "sod_small": ("sod_shock_tube_18432", "cubic", "hydro_av"),
+}
+
+
+def make_workload(args, precision):
+    from spearhed_b200 import setups
+    if args.workload == "orszag_tang":
+        return setups.orszag_tang(nx=args.nx, nz=args.nz, precision=precision)
+    if args.workload == "kelvin_helmholtz":
+        return setups.kelvin_helmholtz(precision=precision)
+    if args.workload == "mhd_rotor":
+        return setups.mhd_rotor(precision=precision)
+    if args.workload == "brio_wu_ensemble":
+        return setups.brio_wu_ensemble(precision=precision)
+    return setups.sod_small(precision=precision)
 
 
 # ------------------------------------------------------------------ clocks
@@ -206,7 +233,8 @@ def run_ours(args, rank, world):
     L.sphx_fma_tflops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.sphx_launch_count.restype = C.c_ulonglong
 
-    w = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
+    wl_name, wl_kernel, wl_phys = WORKLOADS[args.workload]
+    w = make_workload(args, abi.PREC_FP32_COMP)
     w.params.device = dev
     n = w.n
     ctx = sb.context_for(w)
@@ -240,7 +268,7 @@ def run_ours(args, rank, world):
         dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
         dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
         ms_total, pairs = float(mx[0]), float(t[1])
-    passes = flops.PASSES_PER_STEP["mhd"]
+    passes = flops.PASSES_PER_STEP[wl_phys]
     value = passes * pairs / (ms_total * 1e-3)
     ms_step = ms_total / args.steps
 
@@ -252,26 +280,31 @@ def run_ours(args, rank, world):
     L.sphx_fma_tflops(dev, 0, C.byref(peak))
     peak64 = C.c_double(0)
     L.sphx_fma_tflops(dev, 1, C.byref(peak64))
-    force_flops = flops.FORCE_FLOPS["mhd"] * pairs_step
+    force_flops = flops.FORCE_FLOPS[wl_phys] * pairs_step
     achieved = force_flops / (force_ms * 1e-3) / 1e12
-    dens_achieved = flops.DENSITY_FLOPS["wendland_c2"] * pairs_step / (dens_ms * 1e-3) / 1e12
-    traffic = traffic_from_profiles("force_mhd_fp32_orszag_tang.txt")
+    dens_achieved = flops.DENSITY_FLOPS[wl_kernel] * pairs_step / (dens_ms * 1e-3) / 1e12
+    traffic = traffic_from_profiles(f"force_{wl_phys}_fp32_{args.workload}.txt")
     result = {}
     if rank == 0:
         # ---- FP64 plain, same workload, same GPU
-        w64 = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP64)
-        w64.params.device = dev
-        ctx64 = sb.context_for(w64)
-        ctx64.step(args.warmup)
-        e0 = ctx64.reduce()
-        ctx64.step(args.fp64_steps)
-        t64 = ctx64.timings()
-        e1 = ctx64.reduce()
-        v64 = passes * (e1["pairs_total"] - e0["pairs_total"]) / (t64[4] * 1e-3)
-        ctx64.close()
+        ctx.close()
+        if args.workload == "brio_wu_ensemble":
+            # the baseline of the ensemble: the FP64 single-box step looped over boxes
+            v64, t64 = fp64_box_loop(args, dev, passes)
+        else:
+            w64 = make_workload(args, abi.PREC_FP64)
+            w64.params.device = dev
+            ctx64 = sb.context_for(w64)
+            ctx64.step(args.warmup)
+            e0 = ctx64.reduce()
+            ctx64.step(args.fp64_steps)
+            t64 = ctx64.timings()
+            e1 = ctx64.reduce()
+            v64 = passes * (e1["pairs_total"] - e0["pairs_total"]) / (t64[4] * 1e-3)
+            ctx64.close()
         # ---- errors of the FP32 step against the FP64 step from the same state
-        wa = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
-        wb = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP64)
+        wa = make_workload(args, abi.PREC_FP32_COMP)
+        wb = make_workload(args, abi.PREC_FP64)
         ca, cb = sb.context_for(wa), sb.context_for(wb)
         ca.step(1)
         cb.step(1)
@@ -282,7 +315,7 @@ def run_ours(args, rank, world):
         ca.close()
         cb.close()
         # ---- end to end through the C ABI with pinned host buffers
-        wi = setups.orszag_tang(nx=args.nx, nz=args.nz, precision=abi.PREC_FP32_COMP)
+        wi = make_workload(args, abi.PREC_FP32_COMP)
         cols_in = ["pos", "vel", "mass", "h", "density", "u", "B", "psi"]
         cols_out = ["pos", "vel", "density", "u", "B", "psi"]
         # one set of pinned host columns: each step sends them and reads the
@@ -320,15 +353,18 @@ def run_ours(args, rank, world):
         d2h = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_out) * 8 * n
         # ---- CPU baseline (rank 0, N = 1 only)
         cpu = None
-        if world == 1 and not args.no_cpu:
+        if world == 1 and not args.no_cpu and args.workload == "orszag_tang":
             cpu = cpu_reference_sample(args.nx, args.nz)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair kernels (compensated), fp64 integration",
             "data": "synthetic Orszag-Tang initial conditions (lattice, analytic v and B)",
-            "config": {"workload": "orszag_tang_slab_512x512x4", "particles": n, "kernel": "wendland_c2",
-                       "h_over_dx": 1.45, "neighbours_mean": pairs_step / n, "physics": "hydro+AV+SPMHD+Dedner+CFL",
+            "config": {"workload": wl_name if args.workload != "orszag_tang" or args.nx == 512 else
+                       f"orszag_tang_slab_{args.nx}x{args.nx}x{args.nz}", "particles": n, "kernel": wl_kernel,
+                       "boxes": len(w.boxes), "neighbours_mean": pairs_step / n,
+                       "physics": {"mhd": "hydro+AV+SPMHD+Dedner+CFL", "hydro_av": "hydro+AV+CFL"}[wl_phys]
+                       + ("+adaptive_h" if w.params.physics & abi.PHYS_ADAPTIVE_H else ""),
                        "pair_passes_per_step": passes, "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "working set > L2 (lists ~" + f"{n * 4 * 136 / 1e9:.2f}" + " GB, state ~0.3 GB)",
                        "graph": bool(args.graph)},
@@ -342,12 +378,12 @@ def run_ours(args, rank, world):
                                                  "kick_reduce": t64[3] / args.fp64_steps}},
             "error_vs_fp64_after_1_step": {"density_rel_max": err_rho, "accel_normwise": err_acc,
                                            "dBdt_normwise": err_dB},
-            "roofline": {"bound": "fp32_fma", "kernel": "kForce<WendlandC2,float,SPMHD>",
+            "roofline": {"bound": "fp32_fma", "kernel": f"kForce<{wl_kernel},float,{wl_phys}>",
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
-                         "flops_per_pair": flops.FORCE_FLOPS["mhd"], "pairs_per_launch": pairs_step,
+                         "flops_per_pair": flops.FORCE_FLOPS[wl_phys], "pairs_per_launch": pairs_step,
                          "peak_source": "measured live (FMA-chain microbenchmark, sphx_fma_tflops)",
-                         "density_kernel": {"achieved": dens_achieved, "flops_per_pair": flops.DENSITY_FLOPS["wendland_c2"]},
+                         "density_kernel": {"achieved": dens_achieved, "flops_per_pair": flops.DENSITY_FLOPS[wl_kernel]},
                          "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs")},
             "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
@@ -356,8 +392,35 @@ def run_ours(args, rank, world):
         }
         if cpu is not None:
             result["cpu_baseline"] = cpu
-    ctx.close()
     return result
+
+
+def fp64_box_loop(args, dev, passes):
+    """FP64 plain single-box contexts looped over a sample of the ensemble's
+    boxes (the largest and smallest first, then evenly spaced), each for
+    --fp64-steps after --warmup; returns (pair-interactions/s, summed timings)."""
+    import spearhed_b200 as sb
+    from spearhed_b200 import abi, setups
+    import numpy as np
+    # the ensemble's box sizes (same draw as setups.brio_wu_ensemble: Philox key 5)
+    ens_sizes = np.exp(np.random.Generator(np.random.Philox(key=5)).uniform(np.log(4096), np.log(262144), 512)).astype(int)
+    pick = np.linspace(0, len(ens_sizes) - 1, max(1, args.fp64_boxes)).astype(int)
+    pairs = 0.0
+    tm = [0.0] * 5
+    for b in pick:
+        p, box, s = setups.brio_wu_box(int(ens_sizes[b]), precision=abi.PREC_FP64)
+        p.device = dev
+        c = sb.Context(p, [box])
+        c.set_species(abi.SPECIES_DEFAULT, s)
+        c.step(args.warmup)
+        d0 = c.reduce()
+        c.step(args.fp64_steps)
+        t = c.timings()
+        d1 = c.reduce()
+        pairs += d1["pairs_total"] - d0["pairs_total"]
+        tm = [a + x for a, x in zip(tm, t)]
+        c.close()
+    return passes * pairs / (tm[4] * 1e-3), tm
 
 
 def main():

@@ -263,6 +263,7 @@ namespace sph
             T const* sH,
             uint32_t const* sEnt,
             uint32_t m,
+            uint32_t qSelf,
             T supT,
             T R2g,
             uint32_t* list,
@@ -276,11 +277,14 @@ namespace sph
             {
                 // Full chunk: every lane its own target, all lanes read the same
                 // candidate (shared-memory broadcast); bounds are warp-uniform.
+                // The target itself is recognised by its staged index (qSelf, or
+                // ~0 when it is not in this window); entries are read only for
+                // accepted candidates.
+                uint32_t const mySelf = ch.act ? qSelf : 0xffffffffu;
                 uint32_t q0 = 0;
                 for(; q0 + U <= m; q0 += U)
                 {
                     bool acc[U];
-                    uint32_t ent[U];
 #pragma unroll
                     for(int u = 0; u < U; ++u)
                     {
@@ -296,15 +300,14 @@ namespace sph
                             T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
                             R2 = mulRn(R, R);
                         }
-                        ent[u] = sEnt[q0 + u];
-                        acc[u] = r2 < R2;
+                        acc[u] = r2 < R2 && q0 + u != mySelf;
                     }
 #pragma unroll
                     for(int u = 0; u < U; ++u)
-                        if(acc[u] && ch.act && ent[u] != selfEnt)
+                        if(acc[u] && ch.act)
                         {
                             if(!countOnly && ch.nl < cap)
-                                row[ch.nl] = ent[u];
+                                row[ch.nl] = sEnt[q0 + u];
                             ++ch.nl;
                         }
                 }
@@ -404,9 +407,11 @@ namespace sph
                     uint32_t const e = row[k];
                     uint32_t const j = e >> 5, sl = e & 31u;
                     V4 const pj = ld4(rec.pm + j);
-                    T const dx = ch.own.x - (pj.x + T(stencilOff(sl, 0)) * ex);
-                    T const dy = ch.own.y - (pj.y + T(stencilOff(sl, 1)) * ey);
-                    T const dz = ch.own.z - (pj.z + T(stencilOff(sl, 2)) * ez);
+                    int ox, oy, oz;
+                    slotOffsets(sl, ox, oy, oz);
+                    T const dx = ch.own.x - (pj.x + T(ox) * ex);
+                    T const dy = ch.own.y - (pj.y + T(oy) * ey);
+                    T const dz = ch.own.z - (pj.z + T(oz) * ez);
                     T const r2 = dx * dx + dy * dy + dz * dz;
                     T const r = r2 > T(0) ? r2 * rsqrtT(r2) : T(0);
                     rho.add(pj.w * kernelW<K, T>(r, hk));
@@ -570,9 +575,19 @@ namespace sph
                         }
                         __syncwarp();
                         uint32_t const m = ce - cb;
-                        cullChunk<V4, T, PAIRMAX>(A, sPos, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                        // staged index of a target = centre slot's window offset + its rank in the cell
+                        uint32_t const cPre = __shfl_sync(0xffffffffu, pre, kCentreSlot);
+                        uint32_t const cBeg = __shfl_sync(0xffffffffu, sBeg, kCentreSlot);
+                        auto selfIndex = [&](uint32_t t) -> uint32_t
+                        {
+                            uint32_t const q = cPre + (t - cBeg);
+                            return (q >= cb && q < ce) ? q - cb : 0xffffffffu;
+                        };
+                        cullChunk<V4, T, PAIRMAX>(
+                            A, sPos, sH, sEnt, m, selfIndex(A.t), supT, R2g, c.lists.list, cap, countOnly);
                         if(twoChunks)
-                            cullChunk<V4, T, PAIRMAX>(Bc, sPos, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                            cullChunk<V4, T, PAIRMAX>(
+                                Bc, sPos, sH, sEnt, m, selfIndex(Bc.t), supT, R2g, c.lists.list, cap, countOnly);
                     }
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
@@ -639,12 +654,15 @@ namespace sph
                 T vsig = ti.z;
                 uint32_t const n = min(c.lists.count[t], c.lists.cap);
                 uint32_t const* row = c.lists.list + size_t(t) * c.lists.cap;
-                // software pipeline: records of entry k+1 are in flight while k is used
+                // software pipeline: records of entry k+1 are in flight while k is used;
+                // list entries arrive four at a time (rows are 32-byte aligned)
+                uint4 const* row4 = reinterpret_cast<uint4 const*>(row);
+                uint4 ebuf = n > 0 ? row4[0] : make_uint4(0, 0, 0, 0);
                 V4 npm{}, nfv{}, nft{}, nfb{};
                 uint32_t nslot = 0;
                 if(n > 0)
                 {
-                    uint32_t const e = row[0];
+                    uint32_t const e = ebuf.x;
                     uint32_t const j = e >> 5;
                     nslot = e & 31u;
                     npm = ld4(rec.pm + j);
@@ -663,7 +681,11 @@ namespace sph
                         uint32_t const sl = nslot;
                         if(k + 1 < n)
                         {
-                            uint32_t const e = row[k + 1];
+                            uint32_t const k1n = k + 1;
+                            if((k1n & 3u) == 0)
+                                ebuf = row4[k1n >> 2];
+                            uint32_t const sel = k1n & 3u;
+                            uint32_t const e = sel == 0 ? ebuf.x : (sel == 1 ? ebuf.y : (sel == 2 ? ebuf.z : ebuf.w));
                             uint32_t const j = e >> 5;
                             nslot = e & 31u;
                             npm = ld4(rec.pm + j);
@@ -672,9 +694,11 @@ namespace sph
                             if constexpr(PH == 2)
                                 nfb = ld4(rec.fb + j);
                         }
-                        T const rx = pi.x - (pj.x + T(stencilOff(sl, 0)) * ex);
-                        T const ry = pi.y - (pj.y + T(stencilOff(sl, 1)) * ey);
-                        T const rz = pi.z - (pj.z + T(stencilOff(sl, 2)) * ez);
+                        int ox, oy, oz;
+                        slotOffsets(sl, ox, oy, oz);
+                        T const rx = pi.x - (pj.x + T(ox) * ex);
+                        T const ry = pi.y - (pj.y + T(oy) * ey);
+                        T const rz = pi.z - (pj.z + T(oz) * ez);
                         T const r2 = rx * rx + ry * ry + rz * rz;
                         T invR = T(0), r = T(0);
                         if(r2 > T(0))
@@ -683,18 +707,21 @@ namespace sph
                             r = r2 * invR;
                         }
                         T const si = gradWScalar<K, T>(r, invR, hk);
-                        HConst<T> const hkj = hconstFromInv<K, T>(rcpT(vj.w));
-                        T const sj = gradWScalar<K, T>(r, invR, hkj);
+                        T sj = si; // equal smoothing lengths give the same factor
+                        if(vj.w != vi.w)
+                            sj = gradWScalar<K, T>(r, invR, hconstFromInv<K, T>(rcpT(vj.w)));
                         T const mj = pj.w;
                         T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
                         T const vr = vx * rx + vy * ry + vz * rz;
                         T const msi = mj * si;
                         // Isotropic pressure gradient (HydroForces.hpp:155-166).
                         T f = -mj * (ti.y * si + tj.y * sj);
-                        if(av && vr < T(0))
+                        if(av)
                         {
+                            // branch-free: mu = 0 (no viscosity) for receding pairs
+                            T const vn = vr < T(0) ? vr : T(0);
                             T const hb = T(0.5) * (vi.w + vj.w);
-                            T const mu = divT(hb * vr, r2 + eps * hb * hb);
+                            T const mu = divT(hb * vn, r2 + eps * hb * hb);
                             T const cb = T(0.5) * (ti.z + tj.z);
                             T const rb = T(0.5) * (ti.x + tj.x);
                             T const Pi = divT(-alpha * cb * mu + beta * mu * mu, rb);

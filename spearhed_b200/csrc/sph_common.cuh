@@ -50,6 +50,17 @@ namespace sph
     }
     constexpr int kCentreSlot = 13;
 
+    //! Stencil offsets of a slot with integer ops only (no division).
+    __host__ __device__ __forceinline__ void slotOffsets(uint32_t slot, int& ox, int& oy, int& oz)
+    {
+        uint32_t const z = (slot * 57u) >> 9;       // slot / 9 for slot < 27
+        uint32_t const rem = slot - 9u * z;
+        uint32_t const y = (rem * 11u) >> 5;        // rem / 3 for rem < 9
+        ox = int(rem - 3u * y) - 1;
+        oy = int(y) - 1;
+        oz = int(z) - 1;
+    }
+
     //! A neighbour-list entry: sorted source index (27 bits) and stencil slot (5 bits).
     __host__ __device__ __forceinline__ uint32_t packEntry(uint32_t j, uint32_t slot)
     {

@@ -209,3 +209,99 @@ def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, 
     params.h_max = 0.0
     return Workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: species}, steps=100,
                     meta={"sizes": sizes.tolist(), "seed": seed})
+
+
+def kelvin_helmholtz(n_outer=224, n_band=282, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=3):
+    """Magnetised Kelvin-Helmholtz in the periodic unit cube.
+
+    Band |y - 0.5| < 0.25: rho 2, vx +0.5; outside: rho 1, vx -0.5.  Each region
+    is a lattice whose spacing follows its density (n_band/n_outer ~ 2^(1/3);
+    n_outer = 224, n_band = 282 give 5.62 M + 11.21 M = 16.8 M particles, masses
+    within 0.5% of each other).  Uniform jitter of 0.05 spacing (Philox, key
+    ``seed``), vy = 0.01 sin(4 pi x), P = 2.5, gamma 5/3, Bx = 0.1.  Wendland C2,
+    h = hfact x local spacing (adaptive), AV, SPMHD with Dedner cleaning, CFL.
+    """
+    gamma = 5.0 / 3.0
+    if n_outer % 4 or n_band % 2:
+        raise ValueError("n_outer must be a multiple of 4 and n_band even (whole layers per slab)")
+    lo1 = lattice((0.0, 0.0, 0.0), (1.0, 0.25, 1.0), (n_outer, n_outer // 4, n_outer))
+    lo2 = lattice((0.0, 0.75, 0.0), (1.0, 1.0, 1.0), (n_outer, n_outer // 4, n_outer))
+    band = lattice((0.0, 0.25, 0.0), (1.0, 0.75, 1.0), (n_band, n_band // 2, n_band))
+    d_o, d_b = 1.0 / n_outer, 1.0 / n_band
+    pos_o = np.concatenate([lo1, lo2], axis=1)
+    pos_o = pos_o + 0.05 * d_o * philox_uniform(seed, pos_o.shape)
+    pos_b = band + 0.05 * d_b * philox_uniform(seed + 1000, band.shape)
+    pos = np.concatenate([pos_o, pos_b], axis=1) % 1.0
+    n_o, n = pos_o.shape[1], pos_o.shape[1] + pos_b.shape[1]
+    s = abi.Species(n)
+    s.pos[:] = pos
+    isb = np.arange(n) >= n_o
+    s.mass[:] = np.where(isb, 2.0 * d_b ** 3, 1.0 * d_o ** 3)
+    s.density[:] = np.where(isb, 2.0, 1.0)
+    s.u[:] = 2.5 / ((gamma - 1.0) * s.density)
+    s.h[:] = hfact * np.where(isb, d_b, d_o)
+    s.vel[0] = np.where(isb, 0.5, -0.5)
+    s.vel[1] = 0.01 * np.sin(4 * math.pi * pos[0])
+    s.B[0] = 0.1
+    physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
+               | abi.PHYS_ADAPTIVE_H)
+    params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                physics=physics, gamma=gamma, h0=hfact * d_o, dt=1e-4, cfl=0.3, hfact=hfact,
+                                h_max=1.5 * hfact * d_o)
+    box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (1, 1, 1))
+    return Workload("kelvin_helmholtz", params, [box], {abi.SPECIES_DEFAULT: s}, steps=100,
+                    meta={"n_outer": n_outer, "n_band": n_band})
+
+
+def mhd_rotor(nxy=1024, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=4):
+    """MHD rotor in a thin periodic slab [0,1]^2 x [0, nz/nxy].
+
+    Ambient: rho 1 on an nxy x nxy x nz lattice.  Disc r < 0.1 (centre 0.5, 0.5):
+    rho 10 on a finer lattice (9 layers per nz = 4 ambient layers in z, and the
+    in-plane spacing that makes the number density ten times the ambient one),
+    rigid rotation omega 20, linearly tapered to rest between r = 0.1 and 0.115.
+    P = 1, Bx = 5/sqrt(4 pi), gamma 1.4; jitter 0.05 spacing (Philox, key seed).
+    Equal masses; Wendland C2 with adaptive h (h = hfact (m/rho)^(1/3)), so the
+    neighbour count is even in number but the cell sizes vary tenfold in
+    density: the load-imbalance case.  nxy = 1024 gives about 5.4 M particles.
+    """
+    gamma = 1.4
+    Lz = nz / nxy
+    dxa = 1.0 / nxy
+    amb = lattice((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (nxy, nxy, nz))
+    rr = np.hypot(amb[0] - 0.5, amb[1] - 0.5)
+    amb = amb[:, rr >= 0.1]
+    nzd = int(round(nz * 10 ** (1.0 / 3.0)))
+    nzd += 1 if nzd == nz * 2 else 0
+    # in-plane lattice count per unit length giving ten times the ambient number density
+    nd = int(round(np.sqrt(10.0 * nxy ** 3 * Lz / nzd)))
+    sq = lattice((0.4, 0.4, 0.0), (0.6, 0.6, Lz), (int(round(0.2 * nd)), int(round(0.2 * nd)), nzd))
+    disc = sq[:, np.hypot(sq[0] - 0.5, sq[1] - 0.5) < 0.1]
+    pos = np.concatenate([amb, disc], axis=1)
+    pos = pos + 0.05 * dxa * philox_uniform(seed, pos.shape)
+    pos[0] %= 1.0
+    pos[1] %= 1.0
+    pos[2] %= Lz
+    n = pos.shape[1]
+    s = abi.Species(n)
+    s.pos[:] = pos
+    m = dxa ** 2 * (Lz / nz)  # ambient mass: rho 1 times the ambient cell volume
+    s.mass[:] = m
+    isd = np.arange(n) >= amb.shape[1]
+    s.density[:] = np.where(isd, 10.0, 1.0)
+    s.u[:] = 1.0 / ((gamma - 1.0) * s.density)
+    s.h[:] = hfact * np.cbrt(m / s.density)
+    r = np.hypot(pos[0] - 0.5, pos[1] - 0.5)
+    taper = np.clip((0.115 - r) / 0.015, 0.0, 1.0)
+    omega = np.where(r < 0.1, 20.0, 20.0 * taper)
+    s.vel[0] = -omega * (pos[1] - 0.5)
+    s.vel[1] = omega * (pos[0] - 0.5)
+    s.B[0] = 5.0 / math.sqrt(4 * math.pi)
+    physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
+               | abi.PHYS_ADAPTIVE_H)
+    params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                physics=physics, gamma=gamma, h0=hfact * dxa, dt=1e-5, cfl=0.3, hfact=hfact,
+                                h_max=1.3 * hfact * dxa)
+    box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (1, 1, 1))
+    return Workload("mhd_rotor", params, [box], {abi.SPECIES_DEFAULT: s}, steps=150,
+                    meta={"nxy": nxy, "nz": nz, "n_disc": int(isd.sum())})
