@@ -214,6 +214,106 @@ namespace sph
             lo = lo + olo + e;
         }
 
+        //! Far coordinate written into the staged tail past the last candidate:
+        //! its r^2 overflows (FP32) or dwarfs any cull radius (FP64).
+        constexpr float kFar = 1e30f;
+
+        //! Acceptance mask of 32 staged candidates X/Y/Z[0..31] (negated, shifted
+        //! source positions) for one target: bit 31-u set when candidate u has
+        //! r^2 < R^2.  r^2 is the unfused x, y, z sum of the reference's CPU path;
+        //! the test reads the sign of the exactly rounded r^2 - R^2, which is
+        //! negative exactly when r^2 < R^2, and funnels it into the mask.
+        //! FP32: two candidates per instruction with the paired f32x2 arithmetic
+        //! of sm_100 (round-to-nearest per element, the scalar rounding).
+        template<bool PAIRMAX>
+        __device__ __forceinline__ uint32_t cullMask32(
+            float4 const& own,
+            float hi,
+            float const* X,
+            float const* Y,
+            float const* Z,
+            float const* H,
+            float supT,
+            float R2g)
+        {
+            float2 const ox = make_float2(own.x, own.x);
+            float2 const oy = make_float2(own.y, own.y);
+            float2 const oz = make_float2(own.z, own.z);
+            float2 const nR2 = make_float2(-R2g, -R2g);
+            uint32_t mask = 0;
+#pragma unroll
+            for(int q = 0; q < 32; q += 4)
+            {
+                float4 const xv = *reinterpret_cast<float4 const*>(X + q);
+                float4 const yv = *reinterpret_cast<float4 const*>(Y + q);
+                float4 const zv = *reinterpret_cast<float4 const*>(Z + q);
+                float4 hv{};
+                if constexpr(PAIRMAX)
+                    hv = *reinterpret_cast<float4 const*>(H + q);
+#pragma unroll
+                for(int p = 0; p < 2; ++p)
+                {
+                    float2 const dx = __fadd2_rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
+                    float2 const dy = __fadd2_rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
+                    float2 const dz = __fadd2_rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
+                    float2 const r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+                    float2 nr = nR2;
+                    if constexpr(PAIRMAX)
+                    {
+                        float const h0 = p ? hv.z : hv.x, h1 = p ? hv.w : hv.y;
+                        float2 const R = __fmul2_rn(
+                            make_float2(supT, supT),
+                            make_float2(hi > h0 ? hi : h0, hi > h1 ? hi : h1));
+                        float2 const RR = __fmul2_rn(R, R);
+                        nr = make_float2(-RR.x, -RR.y);
+                    }
+                    float2 const d = __fadd2_rn(r2, nr);
+                    mask = __funnelshift_l(__float_as_uint(d.x), mask, 1);
+                    mask = __funnelshift_l(__float_as_uint(d.y), mask, 1);
+                }
+            }
+            return mask;
+        }
+
+        template<bool PAIRMAX>
+        __device__ __forceinline__ uint32_t cullMask32(
+            D4 const& own,
+            double hi,
+            double const* X,
+            double const* Y,
+            double const* Z,
+            double const* H,
+            double supT,
+            double R2g)
+        {
+            uint32_t mask = 0;
+#pragma unroll 4
+            for(int q = 0; q < 32; q += 2)
+            {
+                double2 const xv = *reinterpret_cast<double2 const*>(X + q);
+                double2 const yv = *reinterpret_cast<double2 const*>(Y + q);
+                double2 const zv = *reinterpret_cast<double2 const*>(Z + q);
+#pragma unroll
+                for(int p = 0; p < 2; ++p)
+                {
+                    double const dx = __dadd_rn(own.x, p ? xv.y : xv.x);
+                    double const dy = __dadd_rn(own.y, p ? yv.y : yv.x);
+                    double const dz = __dadd_rn(own.z, p ? zv.y : zv.x);
+                    double const r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                    double R2 = R2g;
+                    if constexpr(PAIRMAX)
+                    {
+                        double const hj = H[q + p];
+                        double const R = __dmul_rn(supT, hi > hj ? hi : hj);
+                        R2 = __dmul_rn(R, R);
+                    }
+                    double const d = __dsub_rn(r2, R2);
+                    mask = __funnelshift_l(uint32_t(__double2hiint(d)), mask, 1);
+                }
+            }
+            return mask;
+        }
+
         //! Per-lane state of one chunk of up to 32 targets of a cell.
         template<typename V4, typename T>
         struct TargetChunk
@@ -256,10 +356,15 @@ namespace sph
 
         //! Cull the staged candidates [0, m) against one target chunk and append
         //! the accepted entries, in candidate order, to each target's list row.
+        //! The staging holds negated shifted positions (sNX, sNY, sNZ), so
+        //! dx = x_i + (-x_j) is the reference's x_i - x_j, rounding included; the
+        //! window is padded with far candidates up to a multiple of 32.
         template<typename V4, typename T, bool PAIRMAX>
         __device__ __forceinline__ void cullChunk(
             TargetChunk<V4, T>& ch,
-            V4 const* sPos,
+            T const* sNX,
+            T const* sNY,
+            T const* sNZ,
             T const* sH,
             uint32_t const* sEnt,
             uint32_t m,
@@ -270,66 +375,35 @@ namespace sph
             uint32_t cap,
             bool countOnly)
         {
-            constexpr int U = 4;
             uint32_t* const row = list + size_t(ch.t) * cap;
-            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
             if(ch.S == 1)
             {
-                // Full chunk: every lane its own target, all lanes read the same
-                // candidate (shared-memory broadcast); bounds are warp-uniform.
-                // The target itself is recognised by its staged index (qSelf, or
-                // ~0 when it is not in this window); entries are read only for
-                // accepted candidates.
+                // Full chunk: every lane its own target; all lanes read the same
+                // 32 candidates (shared-memory broadcast) and build a 32-bit
+                // acceptance mask, then append the accepted entries.  The target
+                // itself is recognised by its staged index (qSelf, or ~0 when it
+                // is not in this window).
                 uint32_t const mySelf = ch.act ? qSelf : 0xffffffffu;
-                uint32_t q0 = 0;
-                for(; q0 + U <= m; q0 += U)
+                for(uint32_t q0 = 0; q0 < m; q0 += 32)
                 {
-                    bool acc[U];
-#pragma unroll
-                    for(int u = 0; u < U; ++u)
+                    uint32_t mask
+                        = cullMask32<PAIRMAX>(ch.own, ch.hi, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
+                    uint32_t const rel = mySelf - q0;
+                    if(rel < 32u)
+                        mask &= ~(0x80000000u >> rel);
+                    if(!ch.act)
+                        mask = 0;
+                    if(countOnly)
                     {
-                        V4 const pj = sPos[q0 + u];
-                        T const dx = subRn(ch.own.x, pj.x);
-                        T const dy = subRn(ch.own.y, pj.y);
-                        T const dz = subRn(ch.own.z, pj.z);
-                        T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
-                        T R2 = R2g;
-                        if constexpr(PAIRMAX)
-                        {
-                            T const hj = sH[q0 + u];
-                            T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
-                            R2 = mulRn(R, R);
-                        }
-                        acc[u] = r2 < R2 && q0 + u != mySelf;
+                        ch.nl += uint32_t(__popc(mask));
+                        continue;
                     }
-#pragma unroll
-                    for(int u = 0; u < U; ++u)
-                        if(acc[u] && ch.act)
-                        {
-                            if(!countOnly && ch.nl < cap)
-                                row[ch.nl] = sEnt[q0 + u];
-                            ++ch.nl;
-                        }
-                }
-                for(; q0 < m; ++q0)
-                {
-                    V4 const pj = sPos[q0];
-                    T const dx = subRn(ch.own.x, pj.x);
-                    T const dy = subRn(ch.own.y, pj.y);
-                    T const dz = subRn(ch.own.z, pj.z);
-                    T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
-                    T R2 = R2g;
-                    if constexpr(PAIRMAX)
+                    while(mask)
                     {
-                        T const hj = sH[q0];
-                        T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
-                        R2 = mulRn(R, R);
-                    }
-                    uint32_t const e = sEnt[q0];
-                    if(r2 < R2 && ch.act && e != selfEnt)
-                    {
-                        if(!countOnly && ch.nl < cap)
-                            row[ch.nl] = e;
+                        uint32_t const u = uint32_t(__clz(mask));
+                        mask &= 0x7fffffffu >> u;
+                        if(ch.nl < cap)
+                            row[ch.nl] = sEnt[q0 + u];
                         ++ch.nl;
                     }
                 }
@@ -337,6 +411,8 @@ namespace sph
             }
             // Short chunk: S lanes per target test interleaved candidates
             // q = q0 + u*S + sub; ballots keep the candidate order.
+            constexpr int U = 4;
+            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
             int const S = ch.S;
             for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(U * S))
             {
@@ -348,10 +424,9 @@ namespace sph
                     uint32_t const q = q0 + uint32_t(u * S + ch.sub);
                     bool const ok = ch.act && q < m;
                     uint32_t const qq = ok ? q : 0u;
-                    V4 const pj = sPos[qq];
-                    T const dx = subRn(ch.own.x, pj.x);
-                    T const dy = subRn(ch.own.y, pj.y);
-                    T const dz = subRn(ch.own.z, pj.z);
+                    T const dx = addRn(ch.own.x, sNX[qq]);
+                    T const dy = addRn(ch.own.y, sNY[qq]);
+                    T const dz = addRn(ch.own.z, sNZ[qq]);
                     T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
                     T R2 = R2g;
                     if constexpr(PAIRMAX)
@@ -459,10 +534,13 @@ namespace sph
             extern __shared__ __align__(32) unsigned char smem[];
             int const warp = threadIdx.x >> 5;
             int const lane = threadIdx.x & 31;
-            V4* sPos = reinterpret_cast<V4*>(smem) + warp * CAP;
-            T* sH = reinterpret_cast<T*>(smem + size_t(kDensWarps) * CAP * sizeof(V4)) + warp * CAP;
-            uint32_t* sEnt = reinterpret_cast<uint32_t*>(smem + size_t(kDensWarps) * CAP * (sizeof(V4) + sizeof(T)))
-                             + warp * CAP;
+            // per warp: negated shifted x, y, z, smoothing length, list entry
+            T* const sNX = reinterpret_cast<T*>(smem) + warp * CAP;
+            T* const sNY = sNX + kDensWarps * CAP;
+            T* const sNZ = sNY + kDensWarps * CAP;
+            T* const sH = sNZ + kDensWarps * CAP;
+            uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + 4 * kDensWarps * CAP)
+                                   + warp * CAP;
             Records<V4, T> const rec = records<T>(c);
             T const supT = T(Kern<K>::support);
             T const Rg = mulRn(supT, T(pa.h0));
@@ -563,18 +641,26 @@ namespace sph
                             for(uint32_t q = lo + uint32_t(lane); q < hi2; q += 32)
                             {
                                 uint32_t const j = b0 + (q - p0);
-                                V4 pj = ld4(rec.pm + j);
-                                pj.x = addRn(pj.x, sx);
-                                pj.y = addRn(pj.y, sy);
-                                pj.z = addRn(pj.z, sz);
-                                sPos[q - cb] = pj;
+                                V4 const pj = ld4(rec.pm + j);
+                                sNX[q - cb] = -addRn(pj.x, sx);
+                                sNY[q - cb] = -addRn(pj.y, sy);
+                                sNZ[q - cb] = -addRn(pj.z, sz);
                                 sEnt[q - cb] = packEntry(j, uint32_t(sl));
                                 if constexpr(PAIRMAX)
                                     sH[q - cb] = rec.hc[j];
                             }
                         }
-                        __syncwarp();
                         uint32_t const m = ce - cb;
+                        // far candidates up to the next multiple of 32
+                        for(uint32_t q = m + uint32_t(lane); q < ((m + 31u) & ~31u); q += 32)
+                        {
+                            sNX[q] = T(kFar);
+                            sNY[q] = T(kFar);
+                            sNZ[q] = T(kFar);
+                            if constexpr(PAIRMAX)
+                                sH[q] = T(0);
+                        }
+                        __syncwarp();
                         // staged index of a target = centre slot's window offset + its rank in the cell
                         uint32_t const cPre = __shfl_sync(0xffffffffu, pre, kCentreSlot);
                         uint32_t const cBeg = __shfl_sync(0xffffffffu, sBeg, kCentreSlot);
@@ -584,10 +670,11 @@ namespace sph
                             return (q >= cb && q < ce) ? q - cb : 0xffffffffu;
                         };
                         cullChunk<V4, T, PAIRMAX>(
-                            A, sPos, sH, sEnt, m, selfIndex(A.t), supT, R2g, c.lists.list, cap, countOnly);
+                            A, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(A.t), supT, R2g, c.lists.list, cap, countOnly);
                         if(twoChunks)
                             cullChunk<V4, T, PAIRMAX>(
-                                Bc, sPos, sH, sEnt, m, selfIndex(Bc.t), supT, R2g, c.lists.list, cap, countOnly);
+                                Bc, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(Bc.t), supT, R2g, c.lists.list, cap,
+                                countOnly);
                     }
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
@@ -832,8 +919,7 @@ namespace sph
         template<typename T>
         constexpr size_t densitySmem()
         {
-            using V4 = typename PairCfg<T>::V4;
-            return size_t(kDensWarps) * PairCfg<T>::cap * (sizeof(V4) + sizeof(T) + sizeof(uint32_t));
+            return size_t(kDensWarps) * PairCfg<T>::cap * (4 * sizeof(T) + sizeof(uint32_t));
         }
 
         template<int K, typename T>
