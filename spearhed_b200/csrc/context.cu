@@ -468,7 +468,8 @@ int sph_ctx::allocate()
     dc.n = n;
     dc.nbox = nbox;
     int st = SPH_OK;
-    if((st = alloc(dc.boxes, nbox)) || (st = allocMaster(dc.cur)) || (st = allocMaster(dc.alt)))
+    if((st = alloc(dc.boxes, nbox)) || (st = alloc(dc.shift32, size_t(nbox) * 32))
+       || (st = alloc(dc.shift64, size_t(nbox) * 32)) || (st = allocMaster(dc.cur)) || (st = allocMaster(dc.alt)))
         return st;
     for(int a = 0; a < 3 && !st; ++a)
         st = alloc(dc.d.dvdt[a], n);
@@ -550,6 +551,18 @@ int sph_ctx::uploadMirror()
         sizeof(sph::BoxDev) * boxDesc.size(),
         cudaMemcpyHostToDevice,
         stream));
+    std::vector<float4> sh32(boxDesc.size() * 32, float4{0.f, 0.f, 0.f, 0.f});
+    std::vector<sph::D4> sh64(boxDesc.size() * 32, sph::D4{0.0, 0.0, 0.0, 0.0});
+    for(size_t b = 0; b < boxDesc.size(); ++b)
+        for(int sl = 0; sl < 27; ++sl)
+        {
+            sph::BoxDev const& d = boxDesc[b];
+            int const o[3] = {sph::stencilOff(sl, 0), sph::stencilOff(sl, 1), sph::stencilOff(sl, 2)};
+            sh32[b * 32 + sl] = float4{float(o[0]) * d.edgef[0], float(o[1]) * d.edgef[1], float(o[2]) * d.edgef[2], 0.f};
+            sh64[b * 32 + sl] = sph::D4{double(o[0]) * d.edge[0], double(o[1]) * d.edge[1], double(o[2]) * d.edge[2], 0.0};
+        }
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.shift32, sh32.data(), sizeof(float4) * sh32.size(), cudaMemcpyHostToDevice, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.shift64, sh64.data(), sizeof(sph::D4) * sh64.size(), cudaMemcpyHostToDevice, stream));
     sph::StepScalars sc{};
     SPH_CUDA_TRY(cudaMemcpyAsync(dc.scal, &sc, sizeof(sc), cudaMemcpyHostToDevice, stream));
     std::vector<double> dts(boxDesc.size(), p.dt);

@@ -31,8 +31,13 @@ namespace sph
     namespace
     {
         constexpr int kDensWarps = 4;
+#ifndef SPH_DENS_MIN_BLOCKS
+#define SPH_DENS_MIN_BLOCKS 6
+#endif
+        constexpr int kDensMinBlocks = SPH_DENS_MIN_BLOCKS; //!< FP32 density blocks per SM (register cap)
         constexpr int kForceThreads = 128;
-        constexpr int kForceMinBlocks = 5; //!< FP32: caps registers near 100 per thread (20 warps per SM)
+        constexpr int kForceMinBlocks = 5;    //!< FP32 hydro: caps registers near 100 per thread (20 warps per SM)
+        constexpr int kForceMinBlocksMhd = 4; //!< FP32 SPMHD: 128 registers, no spills (16 warps per SM)
         constexpr int kBlock = 8; //!< terms per compensated block
 
         template<typename T>
@@ -63,6 +68,19 @@ namespace sph
             return c.r64;
         }
 
+        template<typename T>
+        __device__ __forceinline__ typename PairCfg<T>::V4 const* shiftTable(DevCtx const& c, int box);
+        template<>
+        __device__ __forceinline__ float4 const* shiftTable<float>(DevCtx const& c, int box)
+        {
+            return c.shift32 + size_t(box) * 32;
+        }
+        template<>
+        __device__ __forceinline__ D4 const* shiftTable<double>(DevCtx const& c, int box)
+        {
+            return c.shift64 + size_t(box) * 32;
+        }
+
         // Unfused arithmetic: the reference's CPU evaluation of the pair geometry.
         __device__ __forceinline__ float mulRn(float a, float b)
         {
@@ -72,10 +90,6 @@ namespace sph
         {
             return __fadd_rn(a, b);
         }
-        __device__ __forceinline__ float subRn(float a, float b)
-        {
-            return __fsub_rn(a, b);
-        }
         __device__ __forceinline__ double mulRn(double a, double b)
         {
             return __dmul_rn(a, b);
@@ -83,10 +97,6 @@ namespace sph
         __device__ __forceinline__ double addRn(double a, double b)
         {
             return __dadd_rn(a, b);
-        }
-        __device__ __forceinline__ double subRn(double a, double b)
-        {
-            return __dsub_rn(a, b);
         }
         __device__ __forceinline__ float rsqrtT(float x)
         {
@@ -322,6 +332,7 @@ namespace sph
             T hi;
             uint32_t t;        //!< sorted target index
             uint32_t nl;       //!< accepted so far (same on every lane of the target's group)
+            uint4 buf;         //!< full chunks: the last (nl mod 4) accepted entries, newest in w
             uint32_t groupBase, groupMask, subBelow;
             int S, sub;
             bool act;
@@ -345,6 +356,7 @@ namespace sph
             ch.act = tt < nt;
             ch.t = tc + tt;
             ch.nl = 0;
+            ch.buf = make_uint4(0, 0, 0, 0);
             ch.own = V4{};
             ch.hi = T(1);
             if(ch.act)
@@ -398,13 +410,16 @@ namespace sph
                         ch.nl += uint32_t(__popc(mask));
                         continue;
                     }
+                    // entries go out four at a time (16-byte stores; rows are
+                    // 32-byte aligned and cap is a multiple of 8)
                     while(mask)
                     {
                         uint32_t const u = uint32_t(__clz(mask));
                         mask &= 0x7fffffffu >> u;
-                        if(ch.nl < cap)
-                            row[ch.nl] = sEnt[q0 + u];
+                        ch.buf = make_uint4(ch.buf.y, ch.buf.z, ch.buf.w, sEnt[q0 + u]);
                         ++ch.nl;
+                        if((ch.nl & 3u) == 0 && ch.nl <= cap)
+                            *reinterpret_cast<uint4*>(row + (ch.nl - 4)) = ch.buf;
                     }
                 }
                 return;
@@ -453,6 +468,23 @@ namespace sph
             }
         }
 
+        //! Writes a full chunk's buffered tail (the last nl mod 4 entries).
+        template<typename V4, typename T>
+        __device__ __forceinline__ void flushChunk(TargetChunk<V4, T> const& ch, uint32_t* list, uint32_t cap)
+        {
+            if(!ch.act || ch.S != 1)
+                return;
+            uint32_t const r = ch.nl & 3u;
+            uint32_t const base = ch.nl - r;
+            uint32_t* const row = list + size_t(ch.t) * cap;
+            // buffered entries base .. base+r-1 sit in buf's last r components
+            uint32_t const e[3] = {r == 3 ? ch.buf.y : (r == 2 ? ch.buf.z : ch.buf.w), r == 3 ? ch.buf.z : ch.buf.w, ch.buf.w};
+#pragma unroll
+            for(uint32_t i = 0; i < 3; ++i)
+                if(i < r && base + i < cap)
+                    row[base + i] = e[i];
+        }
+
         //! Density of one target chunk over its list rows; writes rho, the
         //! count and the force-pass records.  Returns the chunk's max c.
         template<int K, typename V4, typename T>
@@ -461,9 +493,7 @@ namespace sph
             DevCtx const& c,
             Records<V4, T> const& rec,
             PhysArgs const& pa,
-            T ex,
-            T ey,
-            T ez,
+            V4 const* stab,
             uint32_t cap)
         {
             bool const lead = ch.act && ch.sub == 0;
@@ -474,22 +504,71 @@ namespace sph
             if(lead)
                 rho.add(ch.own.w * kernelW<K, T>(T(0), hk));
             int const S = ch.S;
-            uint32_t k = uint32_t(ch.sub);
+            auto term = [&](V4 const& pj, V4 const& o)
+            {
+                T const dx = ch.own.x - (pj.x + o.x);
+                T const dy = ch.own.y - (pj.y + o.y);
+                T const dz = ch.own.z - (pj.z + o.z);
+                T const r2 = dx * dx + dy * dy + dz * dz;
+                T const y = rsqrtT(r2);
+                T const r = r2 > T(0) ? r2 * y : T(0);
+                rho.add(pj.w * kernelW<K, T>(r, hk));
+            };
+            if(S == 1)
+            {
+                // Full chunk: the row four entries at a time, the next source's
+                // record in flight; blocks of 8 terms as below.
+                uint4 const* row4 = reinterpret_cast<uint4 const*>(row);
+                V4 npm{};
+                uint32_t nslot = 0;
+                auto fetch = [&](uint32_t e)
+                {
+                    nslot = e & 31u;
+                    npm = ld4(rec.pm + (e >> 5));
+                };
+                auto step = [&](uint32_t next)
+                {
+                    V4 const pj = npm;
+                    V4 const o = ld4(stab + nslot);
+                    fetch(next);
+                    term(pj, o);
+                };
+                uint4 qc = make_uint4(0, 0, 0, 0);
+                if(n > 0)
+                {
+                    qc = row4[0];
+                    fetch(qc.x);
+                }
+                uint32_t const nFull = n & ~3u;
+                for(uint32_t k0 = 0; k0 < nFull; k0 += 4)
+                {
+                    step(qc.y);
+                    step(qc.z);
+                    step(qc.w);
+                    bool const more = k0 + 4 < n;
+                    uint4 const qn = more ? row4[(k0 >> 2) + 1] : qc;
+                    step(more ? qn.x : qc.w);
+                    if(k0 & 4u)
+                        rho.fold();
+                    qc = qn;
+                }
+                uint32_t const tail = n - nFull;
+                if(tail > 0)
+                {
+                    step(tail > 1 ? qc.y : qc.x);
+                    if(tail > 1)
+                        step(tail > 2 ? qc.z : qc.y);
+                    if(tail > 2)
+                        step(qc.z);
+                }
+            }
+            uint32_t k = S == 1 ? n : uint32_t(ch.sub);
             while(k < n)
             {
                 for(int b = 0; b < kBlock && k < n; ++b, k += uint32_t(S))
                 {
                     uint32_t const e = row[k];
-                    uint32_t const j = e >> 5, sl = e & 31u;
-                    V4 const pj = ld4(rec.pm + j);
-                    int ox, oy, oz;
-                    slotOffsets(sl, ox, oy, oz);
-                    T const dx = ch.own.x - (pj.x + T(ox) * ex);
-                    T const dy = ch.own.y - (pj.y + T(oy) * ey);
-                    T const dz = ch.own.z - (pj.z + T(oz) * ez);
-                    T const r2 = dx * dx + dy * dy + dz * dz;
-                    T const r = r2 > T(0) ? r2 * rsqrtT(r2) : T(0);
-                    rho.add(pj.w * kernelW<K, T>(r, hk));
+                    term(ld4(rec.pm + (e >> 5)), ld4(stab + (e & 31u)));
                 }
                 rho.fold();
             }
@@ -527,7 +606,7 @@ namespace sph
         }
 
         template<int K, typename T, bool PAIRMAX>
-        __global__ void __launch_bounds__(kDensWarps * 32, sizeof(T) == 4 ? 6 : 4) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
+        __global__ void __launch_bounds__(kDensWarps * 32, sizeof(T) == 4 ? kDensMinBlocks : 4) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
         {
             using V4 = typename PairCfg<T>::V4;
             constexpr int CAP = PairCfg<T>::cap;
@@ -613,7 +692,6 @@ namespace sph
                 }
                 uint32_t const pre = incl - sCnt;
                 uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
-                T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
 
                 // Two target chunks (up to 64 targets) share every staged window.
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
@@ -681,10 +759,14 @@ namespace sph
                     pairs += (leadA ? A.nl : 0u) + (leadB ? Bc.nl : 0u);
                     if(countOnly)
                         continue;
-                    __syncwarp();
-                    chMax = fmax(chMax, densityChunk<K>(A, c, rec, pa, ex, ey, ez, cap));
+                    flushChunk(A, c.lists.list, cap);
                     if(twoChunks)
-                        chMax = fmax(chMax, densityChunk<K>(Bc, c, rec, pa, ex, ey, ez, cap));
+                        flushChunk(Bc, c.lists.list, cap);
+                    __syncwarp();
+                    V4 const* const stab = shiftTable<T>(c, box);
+                    chMax = fmax(chMax, densityChunk<K>(A, c, rec, pa, stab, cap));
+                    if(twoChunks)
+                        chMax = fmax(chMax, densityChunk<K>(Bc, c, rec, pa, stab, cap));
                 }
             }
             maxCount = warpMaxU(maxCount);
@@ -702,8 +784,8 @@ namespace sph
         }
 
         //! Physics variants compiled separately: 0 = the reference's inviscid
-        //! hydro, 1 = hydro + viscosity, 2 = SPMHD (viscosity, Dedner and the
-        //! tensile correction switched at run time).
+        //! hydro, 1 = hydro + viscosity, 2 = SPMHD with viscosity, Dedner and the
+        //! tensile correction switched at run time, 3 = SPMHD with all three on.
         //!
         //! Accumulators (compensated in FP32): a (pressure, viscosity and magnetic
         //! force together), D = sum m_j s_i v_ij.r (P dV work, div v and the
@@ -711,11 +793,35 @@ namespace sph
         //! + rho_i^2 (Dedner gradient term) for the induction, and the div B sum.
         //! With the tensile correction the Maxwell-stress force and the Borve term
         //! combine to sum m_j s_j (B_j.r)/(mu0 rho_j^2) (B_j - B_i).
-        //! The next neighbour's records are loaded before the current one is used.
+        //!
+        //! The row is read 16 bytes (four entries) at a time; the records of the
+        //! next entry are in flight while the current one is used.  Entries run in
+        //! row order and the compensated blocks hold 8 terms, as in the density
+        //! pass.
+        template<typename V4, typename T>
+        struct ForceAcc
+        {
+            Acc<T> ax, ay, az, D, duav, tx, ty, tz, divb;
+            T vsig;
+            __device__ __forceinline__ void fold()
+            {
+                ax.fold();
+                ay.fold();
+                az.fold();
+                D.fold();
+                duav.fold();
+                tx.fold();
+                ty.fold();
+                tz.fold();
+                divb.fold();
+            }
+        };
+
         template<int K, typename T, int PH>
-        __global__ void __launch_bounds__(kForceThreads, sizeof(T) == 4 ? kForceMinBlocks : 3) kForce(DevCtx c, PhysArgs pa)
+        __global__ void __launch_bounds__(kForceThreads, sizeof(T) == 4 ? (PH >= 2 ? kForceMinBlocksMhd : kForceMinBlocks) : 3) kForce(DevCtx c, PhysArgs pa)
         {
             using V4 = typename PairCfg<T>::V4;
+            constexpr bool kMhd = PH >= 2;
             Records<V4, T> const rec = records<T>(c);
             uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
             bool const act = t < c.n && isTarget(c.cur.role[t]);
@@ -723,169 +829,169 @@ namespace sph
             int const myBox = t < c.n ? c.cur.box[t] : -1;
             if(act)
             {
-                bool const av = (PH == 1) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
-                bool const dedner = PH == 2 && (pa.physics & SPH_PHYS_DEDNER);
-                bool const tensile = PH == 2 && (pa.physics & SPH_PHYS_TENSILE);
-                BoxDev const& B = c.boxes[c.cur.box[t]];
-                T const ex = edgeOf<T>(B, 0), ey = edgeOf<T>(B, 1), ez = edgeOf<T>(B, 2);
+                bool const av = (PH == 1) || (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
+                bool const dedner = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_DEDNER));
+                bool const tensile = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_TENSILE));
+                V4 const* const stab = shiftTable<T>(c, myBox);
                 V4 const pi = ld4(rec.pm + t);
                 V4 const vi = ld4(rec.fv + t);
                 V4 const ti = ld4(rec.ft + t);
                 V4 bi{};
-                if constexpr(PH == 2)
+                if constexpr(kMhd)
                     bi = ld4(rec.fb + t);
                 HConst<T> const hk = hconst<K, T>(vi.w);
                 T const alpha = T(pa.alpha), beta = T(pa.beta), eps = T(pa.avEps);
                 T const rho2i = ti.x * ti.x;
-                Acc<T> ax, ay, az, D, duav, tx, ty, tz, divb;
-                T vsig = ti.z;
+                ForceAcc<V4, T> A;
+                A.vsig = ti.z;
+
+                // one pair term, records of source j and its image shift o
+                auto pair = [&](V4 const& pj, V4 const& vj, V4 const& tj, V4 const& bj, V4 const& o)
+                {
+                    T const rx = pi.x - (pj.x + o.x);
+                    T const ry = pi.y - (pj.y + o.y);
+                    T const rz = pi.z - (pj.z + o.z);
+                    T const r2 = rx * rx + ry * ry + rz * rz;
+                    T const y = rsqrtT(r2);
+                    T const invR = r2 > T(0) ? y : T(0);
+                    T const r = r2 * invR;
+                    T const si = gradWScalar<K, T>(r, invR, hk);
+                    T sj = si; // equal smoothing lengths give the same factor
+                    if(vj.w != vi.w)
+                        sj = gradWScalar<K, T>(r, invR, hconstFromInv<K, T>(rcpT(vj.w)));
+                    T const mj = pj.w;
+                    T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+                    T const vr = vx * rx + vy * ry + vz * rz;
+                    T const msi = mj * si;
+                    // Isotropic pressure gradient (HydroForces.hpp:155-166).
+                    T f = -mj * (ti.y * si + tj.y * sj);
+                    if(av)
+                    {
+                        // branch-free: mu = 0 (no viscosity) for receding pairs
+                        T const vn = vr < T(0) ? vr : T(0);
+                        T const hb = T(0.5) * (vi.w + vj.w);
+                        T const mu = divT(hb * vn, r2 + eps * hb * hb);
+                        T const cb = T(0.5) * (ti.z + tj.z);
+                        T const rb = T(0.5) * (ti.x + tj.x);
+                        T const Pi = divT(-alpha * cb * mu + beta * mu * mu, rb);
+                        T const g = mj * Pi * T(0.5) * (si + sj);
+                        f -= g;
+                        A.duav.add(T(0.5) * g * vr);
+                    }
+                    T fx = f * rx, fy = f * ry, fz = f * rz;
+                    A.D.add(msi * vr);
+                    T const w = vr * invR;
+                    T const vs = ti.z + tj.z - beta * (w < T(0) ? w : T(0));
+                    A.vsig = vs > A.vsig ? vs : A.vsig;
+                    if constexpr(kMhd)
+                    {
+                        T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
+                        T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
+                        T const cj = mj * sj * Bjr * tj.w;
+                        if(tensile)
+                        {
+                            // stress + Borve: c_i B_i + c_j B_j - B_i (c_i + c_j) = c_j (B_j - B_i)
+                            fx += cj * (bj.x - bi.x);
+                            fy += cj * (bj.y - bi.y);
+                            fz += cj * (bj.z - bi.z);
+                        }
+                        else
+                        {
+                            T const ci = msi * Bir * ti.w;
+                            fx += ci * bi.x + cj * bj.x;
+                            fy += ci * bi.y + cj * bj.y;
+                            fz += ci * bi.z + cj * bj.z;
+                        }
+                        T const wB = msi * Bir;
+                        T gx = wB * vx, gy = wB * vy, gz = wB * vz;
+                        if(dedner)
+                        {
+                            // rho_i^2 * m_j (psi_i/rho_i^2 s_i + psi_j/rho_j^2 s_j) r
+                            T const g = rho2i * mj * (bi.w * si + bj.w * sj);
+                            gx += g * rx;
+                            gy += g * ry;
+                            gz += g * rz;
+                        }
+                        A.tx.add(gx);
+                        A.ty.add(gy);
+                        A.tz.add(gz);
+                        A.divb.add(msi * (Bir - Bjr));
+                    }
+                    A.ax.add(fx);
+                    A.ay.add(fy);
+                    A.az.add(fz);
+                };
+
                 uint32_t const n = min(c.lists.count[t], c.lists.cap);
-                uint32_t const* row = c.lists.list + size_t(t) * c.lists.cap;
-                // software pipeline: records of entry k+1 are in flight while k is used;
-                // list entries arrive four at a time (rows are 32-byte aligned)
-                uint4 const* row4 = reinterpret_cast<uint4 const*>(row);
-                uint4 ebuf = n > 0 ? row4[0] : make_uint4(0, 0, 0, 0);
+                // rows are 32-byte aligned and hold a multiple of 8 entries
+                uint4 const* row4 = reinterpret_cast<uint4 const*>(c.lists.list + size_t(t) * c.lists.cap);
                 V4 npm{}, nfv{}, nft{}, nfb{};
                 uint32_t nslot = 0;
-                if(n > 0)
+                auto fetch = [&](uint32_t e)
                 {
-                    uint32_t const e = ebuf.x;
                     uint32_t const j = e >> 5;
                     nslot = e & 31u;
                     npm = ld4(rec.pm + j);
                     nfv = ld4(rec.fv + j);
                     nft = ld4(rec.ft + j);
-                    if constexpr(PH == 2)
+                    if constexpr(kMhd)
                         nfb = ld4(rec.fb + j);
-                }
-                for(uint32_t k0 = 0; k0 < n; k0 += kBlock)
+                };
+                // one entry: take the fetched records, start fetching `next`
+                auto step = [&](uint32_t next)
                 {
-                    uint32_t const k1 = min(n, k0 + kBlock);
-                    for(uint32_t k = k0; k < k1; ++k)
-                    {
-                        V4 const pj = npm, vj = nfv, tj = nft;
-                        V4 const bj = nfb;
-                        uint32_t const sl = nslot;
-                        if(k + 1 < n)
-                        {
-                            uint32_t const k1n = k + 1;
-                            if((k1n & 3u) == 0)
-                                ebuf = row4[k1n >> 2];
-                            uint32_t const sel = k1n & 3u;
-                            uint32_t const e = sel == 0 ? ebuf.x : (sel == 1 ? ebuf.y : (sel == 2 ? ebuf.z : ebuf.w));
-                            uint32_t const j = e >> 5;
-                            nslot = e & 31u;
-                            npm = ld4(rec.pm + j);
-                            nfv = ld4(rec.fv + j);
-                            nft = ld4(rec.ft + j);
-                            if constexpr(PH == 2)
-                                nfb = ld4(rec.fb + j);
-                        }
-                        int ox, oy, oz;
-                        slotOffsets(sl, ox, oy, oz);
-                        T const rx = pi.x - (pj.x + T(ox) * ex);
-                        T const ry = pi.y - (pj.y + T(oy) * ey);
-                        T const rz = pi.z - (pj.z + T(oz) * ez);
-                        T const r2 = rx * rx + ry * ry + rz * rz;
-                        T invR = T(0), r = T(0);
-                        if(r2 > T(0))
-                        {
-                            invR = rsqrtT(r2);
-                            r = r2 * invR;
-                        }
-                        T const si = gradWScalar<K, T>(r, invR, hk);
-                        T sj = si; // equal smoothing lengths give the same factor
-                        if(vj.w != vi.w)
-                            sj = gradWScalar<K, T>(r, invR, hconstFromInv<K, T>(rcpT(vj.w)));
-                        T const mj = pj.w;
-                        T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-                        T const vr = vx * rx + vy * ry + vz * rz;
-                        T const msi = mj * si;
-                        // Isotropic pressure gradient (HydroForces.hpp:155-166).
-                        T f = -mj * (ti.y * si + tj.y * sj);
-                        if(av)
-                        {
-                            // branch-free: mu = 0 (no viscosity) for receding pairs
-                            T const vn = vr < T(0) ? vr : T(0);
-                            T const hb = T(0.5) * (vi.w + vj.w);
-                            T const mu = divT(hb * vn, r2 + eps * hb * hb);
-                            T const cb = T(0.5) * (ti.z + tj.z);
-                            T const rb = T(0.5) * (ti.x + tj.x);
-                            T const Pi = divT(-alpha * cb * mu + beta * mu * mu, rb);
-                            T const g = mj * Pi * T(0.5) * (si + sj);
-                            f -= g;
-                            duav.add(T(0.5) * g * vr);
-                        }
-                        T fx = f * rx, fy = f * ry, fz = f * rz;
-                        D.add(msi * vr);
-                        T const w = vr * invR;
-                        T const vs = ti.z + tj.z - beta * (w < T(0) ? w : T(0));
-                        vsig = vs > vsig ? vs : vsig;
-                        if constexpr(PH == 2)
-                        {
-                            T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
-                            T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
-                            T const cj = mj * sj * Bjr * tj.w;
-                            if(tensile)
-                            {
-                                // stress + Borve: c_i B_i + c_j B_j - B_i (c_i + c_j) = c_j (B_j - B_i)
-                                fx += cj * (bj.x - bi.x);
-                                fy += cj * (bj.y - bi.y);
-                                fz += cj * (bj.z - bi.z);
-                            }
-                            else
-                            {
-                                T const ci = msi * Bir * ti.w;
-                                fx += ci * bi.x + cj * bj.x;
-                                fy += ci * bi.y + cj * bj.y;
-                                fz += ci * bi.z + cj * bj.z;
-                            }
-                            T const wB = msi * Bir;
-                            T gx = wB * vx, gy = wB * vy, gz = wB * vz;
-                            if(dedner)
-                            {
-                                // rho_i^2 * m_j (psi_i/rho_i^2 s_i + psi_j/rho_j^2 s_j) r
-                                T const g = rho2i * mj * (bi.w * si + bj.w * sj);
-                                gx += g * rx;
-                                gy += g * ry;
-                                gz += g * rz;
-                            }
-                            tx.add(gx);
-                            ty.add(gy);
-                            tz.add(gz);
-                            divb.add(msi * (Bir - Bjr));
-                        }
-                        ax.add(fx);
-                        ay.add(fy);
-                        az.add(fz);
-                    }
-                    ax.fold();
-                    ay.fold();
-                    az.fold();
-                    D.fold();
-                    duav.fold();
-                    if constexpr(PH == 2)
-                    {
-                        tx.fold();
-                        ty.fold();
-                        tz.fold();
-                        divb.fold();
-                    }
+                    V4 const pj = npm, vj = nfv, tj = nft, bj = nfb;
+                    V4 const o = ld4(stab + nslot);
+                    fetch(next);
+                    pair(pj, vj, tj, bj, o);
+                };
+                uint4 qc = make_uint4(0, 0, 0, 0);
+                if(n > 0)
+                {
+                    qc = row4[0];
+                    fetch(qc.x);
                 }
+                uint32_t const nFull = n & ~3u;
+                uint32_t k0 = 0;
+                for(; k0 < nFull; k0 += 4)
+                {
+                    step(qc.y);
+                    step(qc.z);
+                    step(qc.w);
+                    // the next quad starts inside the row when k0 + 4 < n
+                    bool const more = k0 + 4 < n;
+                    uint4 const qn = more ? row4[(k0 >> 2) + 1] : qc;
+                    step(more ? qn.x : qc.w); // a valid index either way
+                    if(k0 & 4u)
+                        A.fold();
+                    qc = qn;
+                }
+                // tail: the first n - nFull entries of qc, its first already fetched
+                uint32_t const tail = n - nFull;
+                if(tail > 0)
+                {
+                    step(tail > 1 ? qc.y : qc.x);
+                    if(tail > 1)
+                        step(tail > 2 ? qc.z : qc.y);
+                    if(tail > 2)
+                        step(qc.z);
+                }
+                A.fold();
+
                 // Epilogue in FP64.
                 double const rho = c.cur.rho[t];
                 double const h = c.cur.h[t];
                 double const pr2 = (pa.gamma - 1.0) * c.cur.u[t] / rho; // P_i / rho_i^2
-                double const a[3] = {ax.value(), ay.value(), az.value()};
-                double const Dv = D.value();
-                c.d.dudt[t] = pr2 * Dv + duav.value();
-                if constexpr(PH == 2)
+                double const a[3] = {A.ax.value(), A.ay.value(), A.az.value()};
+                double const Dv = A.D.value();
+                c.d.dudt[t] = pr2 * Dv + A.duav.value();
+                if constexpr(kMhd)
                 {
                     double const Bi[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
                     double const psi = c.cur.psi[t];
-                    double const tv[3] = {tx.value(), ty.value(), tz.value()};
+                    double const tv[3] = {A.tx.value(), A.ty.value(), A.tz.value()};
                     double const invRho = 1.0 / rho;
-                    double const divB = -invRho * divb.value();
+                    double const divB = -invRho * A.divb.value();
                     double const divv = -invRho * Dv;
                     double const ch = __longlong_as_double(static_cast<long long>(c.bs.chBits[myBox]));
                     // dB/dt = -(1/rho)(T_induction - B_i D) - rho grad(psi); T carries rho^2 grad(psi)/rho.
@@ -898,7 +1004,7 @@ namespace sph
 #pragma unroll
                 for(int q = 0; q < 3; ++q)
                     c.d.dvdt[q][t] = a[q];
-                double dt = pa.cfl * h / double(vsig);
+                double dt = pa.cfl * h / double(A.vsig);
                 double const amag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
                 if(amag > 0.0 && pa.cflForce > 0.0)
                     dt = fmin(dt, pa.cflForce * sqrt(h / amag));
@@ -957,7 +1063,13 @@ namespace sph
             unsigned const g = (c.n + kForceThreads - 1) / kForceThreads;
             if(!g)
                 return;
-            if(pa.physics & SPH_PHYS_MHD)
+            uint32_t const full = SPH_PHYS_MHD | SPH_PHYS_AV | SPH_PHYS_DEDNER | SPH_PHYS_TENSILE;
+            if((pa.physics & full) == full)
+            {
+                kForce<K, T, 3><<<g, kForceThreads, 0, s>>>(c, pa);
+                countLaunches(1);
+            }
+            else if(pa.physics & SPH_PHYS_MHD)
             {
                 kForce<K, T, 2><<<g, kForceThreads, 0, s>>>(c, pa);
                 countLaunches(1);

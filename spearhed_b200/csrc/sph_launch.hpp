@@ -176,6 +176,10 @@ namespace sph
         uint32_t n;
         uint32_t nbox;
         BoxDev* boxes;
+        //! Per box, 32 entries: stencil slot s -> image shift (o_x e_x, o_y e_y, o_z e_z, 0)
+        //! with o = the slot's offsets in {-1, 0, 1} and e = the cell edges (exact products).
+        float4* shift32;
+        D4* shift64;
         Master cur, alt;
         Derivs d;
         Cells cells;
