@@ -171,6 +171,7 @@ typedef struct SphDiag
     int64_t steps;         /* steps taken by this context                                   */
     int64_t n_targets;     /* particles in the sums                                         */
     double pairs_total;    /* accepted ordered pairs summed over every step's neighbour build */
+    double candidates;     /* (target, staged source) pairs the cull tested in the last build */
 } SphDiag;
 
 typedef struct sph_ctx sph_ctx;

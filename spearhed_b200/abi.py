@@ -103,6 +103,7 @@ class SphDiag(C.Structure):
         ("steps", C.c_int64),
         ("n_targets", C.c_int64),
         ("pairs_total", C.c_double),
+        ("candidates", C.c_double),
     ]
 
     def as_dict(self):

@@ -677,6 +677,7 @@ int sph_ctx::build(bool drift)
 {
     SPH_CUDA_TRY(cudaMemsetAsync(dc.status, 0, sizeof(uint32_t) * sph::kStatWords, stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
+    SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->candidates, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, sizeof(unsigned long long) * dc.nbox, stream));
     sph::launchDriftKeys(dc, drift, stream);
     bool const inB = sph::radixSortPairs(dc.keysA, dc.valsA, dc.keysB, dc.valsB, n, dc.keyBits, dc.sortScratch, stream);
@@ -1007,6 +1008,7 @@ int sph_density(sph_ctx* ctx)
             return st;
         SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.status, 0, sizeof(uint32_t) * sph::kStatWords, ctx->stream));
         SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->pairs, 0, sizeof(unsigned long long), ctx->stream));
+        SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->candidates, 0, sizeof(unsigned long long), ctx->stream));
         SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.bs.chBits, 0, sizeof(unsigned long long) * ctx->dc.nbox, ctx->stream));
         if((st = ctx->densityPass()) || (st = ctx->checkStatus("sph_density")))
             return st;
@@ -1181,6 +1183,7 @@ namespace
         o.pairs = double(sc.pairs);
         o.steps = sc.steps;
         o.pairs_total = sc.pairsAccum;
+        o.candidates = double(sc.candidates);
     }
 } // namespace
 

@@ -628,6 +628,7 @@ namespace sph
             uint32_t const nWarps = gridDim.x * kDensWarps;
             uint32_t maxCount = 0;
             unsigned long long pairs = 0;
+            unsigned long long cand = 0; // warp-uniform: staged sources x targets culled
             double chMax = 0.0;
             int chBox = -1; // box whose c_h maximum chMax holds (warp-uniform)
 
@@ -754,6 +755,7 @@ namespace sph
                                 Bc, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(Bc.t), supT, R2g, c.lists.list, cap,
                                 countOnly);
                     }
+                    cand += uint64_t(total) * (min(32u, tEnd - tc) + (twoChunks ? min(32u, tEnd - tc - 32) : 0u));
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
                     pairs += (leadA ? A.nl : 0u) + (leadB ? Bc.nl : 0u);
@@ -778,6 +780,7 @@ namespace sph
                     atomicMax(&c.status[kStatOverflow], maxCount);
                 atomicMax(&c.status[kStatMaxCount], maxCount);
                 atomicAdd(&c.scal->pairs, pairs);
+                atomicAdd(&c.scal->candidates, cand);
                 if(!countOnly && chBox >= 0)
                     atomicMax(&c.bs.chBits[chBox], orderedBits(chMax));
             }

@@ -157,6 +157,7 @@ namespace sph
         unsigned long long pairs;  //!< accepted ordered pairs of the last neighbour build
         double pairsAccum;         //!< accepted pairs summed over the steps taken
         long long steps;
+        unsigned long long candidates; //!< (target, staged source) pairs tested by the last cull
     };
 
     //! Per-box step state (structure of arrays, nbox entries each).  Boxes of an

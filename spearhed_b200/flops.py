@@ -3,9 +3,11 @@
 Counting rule: one FP32 (or FP64) add, multiply, compare-select or min/max is 1
 flop; a fused multiply-add is 2; a reciprocal square root, reciprocal or
 division is 1.  Candidate tests that are rejected by the cull are not counted
-(they are reported separately as cull efficiency), and the artificial-viscosity
-branch, taken only by approaching pairs, is not counted either, so the figures
-are lower bounds.
+(they are reported separately as cull efficiency, CULL_FLOPS_PER_CANDIDATE each),
+and the artificial-viscosity terms, evaluated branch-free for every pair but
+nonzero only for approaching ones, are not counted either, so the figures are
+lower bounds.  s_j is counted even where equal smoothing lengths let the kernel
+reuse s_i.
 
 Wendland C2 kernel (the benchmark workload's kernel):
   density pass, per accepted pair (pair_kernels.cu, kDensity sum over the list):
@@ -16,7 +18,7 @@ Wendland C2 kernel (the benchmark workload's kernel):
        sigma/h^3 * (1)                                            9
     m_j * W and accumulate (fma)                                  2
                                                                  27
-  force pass, SPMHD variant, per accepted pair (kForce<K, T, 2>):
+  force pass, SPMHD variant, per accepted pair (kForce<K, T, 2 or 3>):
     displacement + r^2 + rsqrt + r                               16
     s_i: x (1), shape (6), dwnorm * shape * invR (2)              9
     s_j: 1/h_j (1), h-powers and norms (4), x (1), shape (6), (2) 14
@@ -44,3 +46,6 @@ FORCE_FLOPS = {  # by physics variant
     "mhd": 115,
 }
 PASSES_PER_STEP = {"hydro": 2, "hydro_av": 2, "mhd": 3}
+# cull test of one (target, staged source) candidate: 3 differences, 3 squares,
+# 2 adds for r^2 and the r^2 - R^2 whose sign is the acceptance bit
+CULL_FLOPS_PER_CANDIDATE = 9
