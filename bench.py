@@ -213,11 +213,13 @@ class ClockSampler:
 
 # ------------------------------------------------------------- helpers
 def pinned_species(src, fields):
-    """A Species whose listed columns live in pinned host memory (torch)."""
+    """A Species whose listed columns live in pinned host memory (torch); the
+    box ids are carried over as they are."""
     import torch
 
     from spearhed_b200 import abi
     s = abi.Species(src.n)
+    s.box_id = src.box_id.copy()
     for f in fields:
         a = getattr(src, f)
         t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
@@ -352,6 +354,15 @@ def run_ours(args, rank, world):
     L.sphx_fma_tflops(dev, 0, C.byref(peak))
     peak64 = C.c_double(0)
     L.sphx_fma_tflops(dev, 1, C.byref(peak64))
+    if force_ms <= 0 or dens_ms <= 0:
+        # graph replay records no per-stage events: time one eager step for the
+        # per-kernel figures and stage shares (the headline value stays graph-timed)
+        ctx.use_graph(False)
+        ctx.step(1)
+        ts = ctx.timings()
+        ctx.use_graph(True)
+        dens_ms, force_ms = ts[1], ts[2]
+        tm = [ts[k] * args.steps for k in range(4)] + [tm[4]]
     force_achieved = flops.FORCE_FLOPS[wl_phys] * pairs_step / (force_ms * 1e-3) / 1e12
     dens_achieved = flops.DENSITY_FLOPS[wl_kernel] * pairs_step / (dens_ms * 1e-3) / 1e12
     cull_achieved = flops.CULL_FLOPS_PER_CANDIDATE * cand_step / (dens_ms * 1e-3) / 1e12
@@ -396,7 +407,8 @@ def run_ours(args, rank, world):
         ga, gb = ca.get_species(0), cb.get_species(0)
         err_rho = float(np.max(np.abs(ga.density / gb.density - 1.0)))
         err_acc = float(np.max(np.abs(ga.dvdt - gb.dvdt)) / np.max(np.abs(gb.dvdt)))
-        err_dB = float(np.max(np.abs(ga.dBdt - gb.dBdt)) / np.max(np.abs(gb.dBdt)))
+        dBmax = float(np.max(np.abs(gb.dBdt)))
+        err_dB = float(np.max(np.abs(ga.dBdt - gb.dBdt)) / dBmax) if dBmax > 0 else None
         ca.close()
         cb.close()
         # ---- end to end through the C ABI with pinned host buffers

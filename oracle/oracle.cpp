@@ -324,7 +324,21 @@ namespace orc
                     hgrid = s.p.h_max;
                 }
                 else if(s.p.physics & SPH_PHYS_ADAPTIVE_H)
-                    hgrid = 1.5 * hmax[b];
+                {
+                    // room to grow, clipped where a periodic axis would fall
+                    // below one cull radius (the kick caps h at hcap)
+                    double grow = 1.5 * hmax[b];
+                    for(int a = 0; a < 3; ++a)
+                        if(s.boxes[b].periodic[a])
+                        {
+                            double const L = s.boxes[b].hi[a] - s.boxes[b].lo[a];
+                            double lim = L / (double(sup) * (1.0 + 1.0 / 262144.0));
+                            while(lim > hmax[b] && cellRadius(sup, lim) > L)
+                                lim = std::nextafter(lim, 0.0);
+                            grow = std::min(grow, lim);
+                        }
+                    hgrid = std::max(hmax[b], grow);
+                }
             }
             s.hcap[b] = hgrid;
             int const st = makeGrid(s.boxes[b], cellRadius(sup, hgrid), s.grids[b]);

@@ -175,13 +175,22 @@ struct sph_ctx
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
     int parity = 0;
     std::vector<cudaEvent_t> events;
+    cudaEvent_t eCall = nullptr; //!< start of a step call (before its snapshot)
     double timings[5] = {0, 0, 0, 0, 0};
+    // State a step call starts from, restored when a neighbour list overflowed
+    // in any of its steps: the call then regrows the lists and runs again.
+    bool haveSnap = false;
+    sph::Master snap{};
+    sph::BoxScalars snapBs{};
+    sph::StepScalars* snapScal = nullptr;
 
     ~sph_ctx()
     {
         release();
         for(cudaEvent_t e : events)
             cudaEventDestroy(e);
+        if(eCall)
+            cudaEventDestroy(eCall);
         if(stream)
             cudaStreamDestroy(stream);
     }
@@ -208,6 +217,10 @@ struct sph_ctx
         dc = sph::DevCtx{};
         boxOut = nullptr;
         boxScratch = nullptr;
+        haveSnap = false;
+        snap = sph::Master{};
+        snapBs = sph::BoxScalars{};
+        snapScal = nullptr;
         allocated = false;
         deviceCurrent = false;
         densityValid = false;
@@ -332,7 +345,10 @@ struct sph_ctx
     int probeListCapacity();
     int growLists(uint32_t need);
     int build(bool drift);
+    int clearStatus();
     int checkStatus(char const* where);
+    int snapshot(bool restore);
+    int runSteps(int32_t nsteps);
     int densityPass();
     int forcePass();
     int stepOnce(cudaEvent_t const* ev);
@@ -429,7 +445,21 @@ int sph_ctx::layout()
                 hgrid = p.h_max;
             }
             else if(p.physics & SPH_PHYS_ADAPTIVE_H)
-                hgrid = 1.5 * hmax[b];
+            {
+                // room to grow, but never past what a periodic axis admits (the
+                // kick caps h at hcap, so the grid stays valid)
+                double grow = 1.5 * hmax[b];
+                for(int a = 0; a < 3; ++a)
+                    if(B.periodic[a])
+                    {
+                        double const L = B.hi[a] - B.lo[a];
+                        double lim = L / (double(sup) * (1.0 + 1.0 / 262144.0));
+                        while(lim > hmax[b] && cellRadius(sup, lim) > L)
+                            lim = std::nextafter(lim, 0.0);
+                        grow = std::min(grow, lim);
+                    }
+                hgrid = std::max(hmax[b], grow);
+            }
         }
         double const rc = cellRadius(sup, hgrid);
         sph::BoxDev& d = boxDesc[b];
@@ -495,7 +525,8 @@ int sph_ctx::allocate()
     if((st = alloc(dc.keysA, n)) || (st = alloc(dc.valsA, n)) || (st = alloc(dc.keysB, n)) || (st = alloc(dc.valsB, n))
        || (st = alloc(dc.sortScratch, sph::radixScratchWords(n))))
         return st;
-    if((st = alloc(dc.status, sph::kStatWords)) || (st = alloc(dc.scal, 1)) || (st = alloc(dc.diag, sph::kDiagWords)))
+    if((st = alloc(dc.status, sph::kStatWords)) || (st = alloc(dc.scal, 1)) || (st = alloc(dc.diag, sph::kDiagWords))
+       || (st = alloc(dc.work, 1)))
         return st;
     if((st = alloc(dc.bs.dt, nbox)) || (st = alloc(dc.bs.time, nbox)) || (st = alloc(dc.bs.lastDt, nbox))
        || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)))
@@ -609,8 +640,8 @@ int sph_ctx::probeListCapacity()
     uint32_t capN = uint32_t(p.max_neighbours);
     if(capN == 0)
     {
-        int st = build(false);
-        if(st)
+        int st = clearStatus();
+        if(st || (st = build(false)))
             return st;
         sph::launchDensity(dc, pa, p.kernel, p.precision, true, stream);
         uint32_t stat[sph::kStatWords];
@@ -675,7 +706,6 @@ int sph_ctx::ensureDevice()
 //! Drift (optional) + cell keys + sort + cell ranges + permute/pack.
 int sph_ctx::build(bool drift)
 {
-    SPH_CUDA_TRY(cudaMemsetAsync(dc.status, 0, sizeof(uint32_t) * sph::kStatWords, stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->candidates, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, sizeof(unsigned long long) * dc.nbox, stream));
@@ -701,6 +731,52 @@ int sph_ctx::forcePass()
 {
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.dtBits, 0x7f, sizeof(unsigned long long) * dc.nbox, stream));
     sph::launchForce(dc, pa, p.kernel, p.precision, stream);
+    return SPH_OK;
+}
+
+//! Zeroes the status words once per call: non-finite and escaped particles,
+//! list overflow and the largest neighbour count then accumulate over every
+//! step of the call, so a condition raised by any step is reported.
+int sph_ctx::clearStatus()
+{
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.status, 0, sizeof(uint32_t) * sph::kStatWords, stream));
+    return SPH_OK;
+}
+
+//! Saves (restore = false) or restores (restore = true) the state a step call
+//! starts from: every master column of the current buffer, the per-box clock
+//! and CFL/Dedner words, and the step scalars.  The snapshot is allocated on
+//! the first step call and freed with the context.
+int sph_ctx::snapshot(bool restore)
+{
+    uint32_t const nb = dc.nbox;
+    if(!haveSnap)
+    {
+        if(restore)
+            return fail(SPH_ERR_STATE, "no step snapshot to restore");
+        int st = allocMaster(snap);
+        if(st || (st = alloc(snapBs.dt, nb)) || (st = alloc(snapBs.time, nb)) || (st = alloc(snapBs.lastDt, nb))
+           || (st = alloc(snapBs.dtBits, nb)) || (st = alloc(snapBs.chBits, nb)) || (st = alloc(snapScal, 1)))
+            return st;
+        haveSnap = true;
+    }
+    sph::Master const& from = restore ? snap : dc.cur;
+    sph::Master const& to = restore ? dc.cur : snap;
+    sph::BoxScalars const& bf = restore ? snapBs : dc.bs;
+    sph::BoxScalars const& bt = restore ? dc.bs : snapBs;
+    sph::launchCopyMaster(to, from, n, stream);
+    auto const d2d = cudaMemcpyDeviceToDevice;
+    SPH_CUDA_TRY(cudaMemcpyAsync(bt.dt, bf.dt, 8 * size_t(nb), d2d, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(bt.time, bf.time, 8 * size_t(nb), d2d, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(bt.lastDt, bf.lastDt, 8 * size_t(nb), d2d, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(bt.dtBits, bf.dtBits, 8 * size_t(nb), d2d, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(bt.chBits, bf.chBits, 8 * size_t(nb), d2d, stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(
+        restore ? dc.scal : snapScal,
+        restore ? snapScal : dc.scal,
+        sizeof(sph::StepScalars),
+        d2d,
+        stream));
     return SPH_OK;
 }
 
@@ -751,13 +827,53 @@ int sph_ctx::stepOnce(cudaEvent_t const* ev)
     return SPH_OK;
 }
 
+//! n_steps of runOneStep.  The call is transactional with respect to the
+//! neighbour-list capacity: the state it starts from is saved first, and if a
+//! list overflowed in any step (steps run without host round trips, so this is
+//! seen only at the end), the lists grow, the state is restored and the steps
+//! run again.  timings[4] spans the whole call, replays included; the per-stage
+//! times are those of the run that is kept.
 int sph_ctx::steps(int32_t nsteps, double dt)
 {
     int st = ensureDevice();
     if(st)
         return st;
+    if(!eCall)
+        SPH_CUDA_TRY(cudaEventCreate(&eCall));
+    SPH_CUDA_TRY(cudaEventRecord(eCall, stream));
     if(dt > 0.0)
         sph::launchFill(dc.bs.dt, dc.nbox, dt, stream);
+    if((st = snapshot(false)))
+        return st;
+    constexpr int kMaxReplays = 8;
+    for(int attempt = 0;; ++attempt)
+    {
+        st = runSteps(nsteps);
+        if(st != SPH_ERR_OVERFLOW || attempt == kMaxReplays)
+            break;
+        uint32_t stat[sph::kStatWords];
+        SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
+        int const g = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16);
+        if(g)
+            return g;
+        if((st = snapshot(true)))
+            return st;
+    }
+    float ms = 0.f;
+    if(cudaEventElapsedTime(&ms, eCall, events[1]) == cudaSuccess)
+        timings[4] = ms;
+    densityValid = st == SPH_OK;
+    forceValid = st == SPH_OK;
+    return st;
+}
+
+//! One attempt of a step call: the steps (pairs of them as CUDA graphs when
+//! enabled), then the status check.
+int sph_ctx::runSteps(int32_t nsteps)
+{
+    int st = clearStatus();
+    if(st)
+        return st;
     for(double& t : timings)
         t = 0.0;
     bool const graph = useGraph && nsteps >= 2;
@@ -810,17 +926,6 @@ int sph_ctx::steps(int32_t nsteps, double dt)
                 cudaEventElapsedTime(&ms, events[2 + size_t(s) * 5 + k], events[2 + size_t(s) * 5 + k + 1]);
                 timings[k] += ms;
             }
-    densityValid = true;
-    forceValid = true;
-    if(st == SPH_ERR_OVERFLOW)
-    {
-        // The lists grow for the next call; this call's result is not valid.
-        uint32_t stat[sph::kStatWords];
-        SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
-        int const g = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16);
-        if(g)
-            return g;
-    }
     return st;
 }
 
@@ -997,7 +1102,7 @@ int sph_density(sph_ctx* ctx)
         return fail(SPH_ERR_INVALID, "null context");
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     int st = ctx->ensureDevice();
-    if(st || (st = ctx->build(false)) || (st = ctx->densityPass()))
+    if(st || (st = ctx->clearStatus()) || (st = ctx->build(false)) || (st = ctx->densityPass()))
         return st;
     st = ctx->checkStatus("sph_density");
     if(st == SPH_ERR_OVERFLOW)

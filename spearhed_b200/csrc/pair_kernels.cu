@@ -625,15 +625,22 @@ namespace sph
             T const Rg = mulRn(supT, T(pa.h0));
             T const R2g = mulRn(Rg, Rg);
             uint32_t const cap = c.lists.cap;
-            uint32_t const nWarps = gridDim.x * kDensWarps;
             uint32_t maxCount = 0;
             unsigned long long pairs = 0;
             unsigned long long cand = 0; // warp-uniform: staged sources x targets culled
             double chMax = 0.0;
             int chBox = -1; // box whose c_h maximum chMax holds (warp-uniform)
 
-            for(uint32_t cell = blockIdx.x * kDensWarps + warp; cell < c.cells.ncells; cell += nWarps)
+            // Work queue: each warp takes its next cell from a counter; the fetch
+            // for the next cell is issued first and read at the loop's end.
+            uint32_t pending = 0;
+            if(lane == 0)
+                pending = atomicAdd(c.work, 1u);
+            for(uint32_t cell = __shfl_sync(0xffffffffu, pending, 0); cell < c.cells.ncells;
+                cell = __shfl_sync(0xffffffffu, pending, 0))
             {
+                if(lane == 0)
+                    pending = atomicAdd(c.work, 1u);
                 uint32_t const tBeg = c.cells.start[cell];
                 uint32_t const tEnd = c.cells.mid[cell];
                 if(tBeg >= tEnd)
@@ -1042,10 +1049,14 @@ namespace sph
         void densityOne(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
         {
             size_t const smem = densitySmem<T>();
+            // persistent grid: enough resident blocks to fill every SM; cells come
+            // from the work queue
             uint32_t blocks = (c.cells.ncells + kDensWarps - 1) / kDensWarps;
-            blocks = blocks > 148u * 64u ? 148u * 64u : blocks;
+            uint32_t const resident = 148u * (sizeof(T) == 4 ? kDensMinBlocks : 4);
+            blocks = blocks > resident ? resident : blocks;
             if(blocks)
             {
+                cudaMemsetAsync(c.work, 0, sizeof(uint32_t), s);
                 kDensity<K, T, PM><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
                 countLaunches(1);
             }

@@ -193,6 +193,7 @@ namespace sph
         uint32_t* valsB;
         uint32_t* sortScratch;
         uint32_t* status; //!< kStatWords words
+        uint32_t* work;   //!< density work queue: next cell to hand out (zeroed before each launch)
         StepScalars* scal;
         BoxScalars bs;
         double* partials; //!< per-block diagnostics partial sums
@@ -235,6 +236,8 @@ namespace sph
     void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, double* scratch, cudaStream_t s);
     size_t boxReduceScratchDoubles(uint32_t nbox);
     void launchFill(double* p, size_t n, double v, cudaStream_t s);
+    //! dst <- src for every master column (n particles).
+    void launchCopyMaster(Master const& dst, Master const& src, uint32_t n, cudaStream_t s);
     //! master[p] = src[id[p]] for one species; badCount (or null) counts values
     //! that are not positive and finite.
     void launchGatherSpecies(

@@ -8,6 +8,7 @@
 // columns in, coalesced columns out.
 #include "sph_launch.hpp"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace sph
@@ -360,6 +361,29 @@ namespace sph
                 p[i] = v;
         }
 
+        //! Copy of every master column (the state a step call starts from).
+        __global__ void kCopyMaster(Master dst, Master src, uint32_t n)
+        {
+            for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+#pragma unroll
+                for(int a = 0; a < 3; ++a)
+                {
+                    dst.x[a][i] = src.x[a][i];
+                    dst.v[a][i] = src.v[a][i];
+                    dst.B[a][i] = src.B[a][i];
+                }
+                dst.u[i] = src.u[i];
+                dst.m[i] = src.m[i];
+                dst.h[i] = src.h[i];
+                dst.rho[i] = src.rho[i];
+                dst.psi[i] = src.psi[i];
+                dst.id[i] = src.id[i];
+                dst.box[i] = src.box[i];
+                dst.role[i] = src.role[i];
+            }
+        }
+
         //! Sorted-particle range [first, last) of every box's sources: one block
         //! per box takes the min start / max end over the box's non-empty cells.
         __global__ void __launch_bounds__(kThreads) kBoxRange(DevCtx c, uint32_t* range)
@@ -600,6 +624,16 @@ namespace sph
         if(n)
         {
             kGatherSpeciesInt<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, master);
+            countLaunches(1);
+        }
+    }
+
+    void launchCopyMaster(Master const& dst, Master const& src, uint32_t n, cudaStream_t s)
+    {
+        if(n)
+        {
+            unsigned const blocks = unsigned(std::min<uint32_t>((n + 255) / 256, 148u * 16u));
+            kCopyMaster<<<blocks, 256, 0, s>>>(dst, src, n);
             countLaunches(1);
         }
     }

@@ -98,3 +98,29 @@ def test_fp64_runs_are_bit_reproducible():
     b, _ = _run(w.params, w.boxes, s.copy(), 5)
     for f in FIELDS:
         assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32_COMP])
+def test_list_overflow_in_a_step_call_replays_from_its_start(prec):
+    """A step call whose lists overflow (capacity forced to 32 entries for 92
+    neighbours) restores the state it started from, regrows the lists and runs
+    again: the result equals a run with large enough lists, bit for bit.  Both
+    contexts get a fixed capacity, so neither runs the sizing pass (which sorts
+    the particles once and so changes the summation order inside cells)."""
+    import spearhed_b200 as sb
+    w = setups.orszag_tang(nx=32, nz=4, precision=prec, jitter=0.1)
+    s = w.species[abi.SPECIES_DEFAULT]
+    w.params.max_neighbours = 256
+    ref, dref = _run(w.params, w.boxes, s.copy(), 5)
+    w.params.max_neighbours = 32
+    ctx = sb.Context(w.params, w.boxes)
+    ctx.set_species(abi.SPECIES_DEFAULT, s.copy())
+    ctx.step(5)
+    got = ctx.get_species(abi.SPECIES_DEFAULT)
+    dg = ctx.reduce()
+    assert int(np.max(ctx.neighbour_counts(abi.SPECIES_DEFAULT))) > 32
+    ctx.close()
+    for f in FIELDS:
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    assert dg["time"] == dref[0]["time"]
+    assert dg["steps"] == dref[0]["steps"] == 5
