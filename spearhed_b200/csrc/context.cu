@@ -794,11 +794,6 @@ int sph_ctx::checkStatus(char const* where)
         return fail(
             SPH_ERR_OUTSIDE,
             std::string(where) + ": " + std::to_string(stat[sph::kStatOutside]) + " particles left a non-periodic box");
-    if(stat[sph::kStatTimeout])
-        return fail(
-            SPH_ERR_CUDA,
-            std::string(where) + ": " + std::to_string(stat[sph::kStatTimeout])
-                + " warps gave up waiting for their shared-memory staging copies");
     if(stat[sph::kStatOverflow])
         return fail(
             SPH_ERR_OVERFLOW,

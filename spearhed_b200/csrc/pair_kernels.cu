@@ -224,62 +224,6 @@ namespace sph
             lo = lo + olo + e;
         }
 
-        // ---- bulk copies global -> shared completing on an mbarrier (sm_90+ PTX,
-        // untiled: 16-byte aligned addresses, sizes a multiple of 16, no multicast)
-        __device__ __forceinline__ uint32_t smemAddr(void const* p)
-        {
-            return uint32_t(__cvta_generic_to_shared(p));
-        }
-        __device__ __forceinline__ void mbarInit(uint64_t* bar)
-        {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        //! The single arrival of a phase, announcing `bytes` of copies.
-        __device__ __forceinline__ void mbarExpectTx(uint64_t* bar, uint32_t bytes)
-        {
-            asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(
-                             smemAddr(bar)),
-                         "r"(bytes)
-                         : "memory");
-        }
-        __device__ __forceinline__ void bulkCopyToShared(void* dst, void const* src, uint32_t bytes, uint64_t* bar)
-        {
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smemAddr(dst)),
-                "l"(src),
-                "r"(bytes),
-                "r"(smemAddr(bar))
-                : "memory");
-        }
-        __device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t parity)
-        {
-            uint32_t ok;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
-                "p;\n}"
-                : "=r"(ok)
-                : "r"(smemAddr(bar)), "r"(parity)
-                : "memory");
-            return ok != 0;
-        }
-        //! Waits for a phase with an iteration limit (each try suspends for a
-        //! bounded time); false when the limit ran out.
-        __device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t parity)
-        {
-            for(uint32_t it = 0; it < (1u << 20); ++it)
-                if(mbarTryWait(bar, parity))
-                    return true;
-            return false;
-        }
-        //! Orders this thread's earlier shared-memory accesses before later
-        //! async-proxy (bulk copy) writes to the same memory.
-        __device__ __forceinline__ void fenceProxyAsync()
-        {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        }
-
         //! Far coordinate written into the staged tail past the last candidate:
         //! its r^2 overflows (FP32) or dwarfs any cull radius (FP64).
         constexpr float kFar = 1e30f;
@@ -676,19 +620,6 @@ namespace sph
             T* const sH = sNZ + kDensWarps * CAP;
             uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + 4 * kDensWarps * CAP)
                                    + warp * CAP;
-            // FP32: the window's raw source records arrive by bulk copies into sRaw
-            // (one copy per stencil slot segment) and complete on the warp's mbarrier
-            constexpr bool kBulk = sizeof(T) == 4;
-            unsigned char* const bulkBase = smem + size_t(kDensWarps) * CAP * (4 * sizeof(T) + sizeof(uint32_t));
-            V4* const sRaw = reinterpret_cast<V4*>(bulkBase) + warp * CAP;
-            uint64_t* const bar = reinterpret_cast<uint64_t*>(bulkBase + size_t(kDensWarps) * CAP * sizeof(V4)) + warp;
-            uint32_t phase = 0;
-            if constexpr(kBulk)
-            {
-                if(lane == 0)
-                    mbarInit(bar);
-                __syncwarp();
-            }
             Records<V4, T> const rec = records<T>(c);
             T const supT = T(Kern<K>::support);
             T const Rg = mulRn(supT, T(pa.h0));
@@ -770,31 +701,6 @@ namespace sph
                 uint32_t const pre = incl - sCnt;
                 uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
 
-                // Bulk copies of window [cb, cb + CAP): one per stencil-slot segment
-                // (contiguous sorted records), issued by lane 0 after announcing
-                // the window's bytes on the mbarrier.
-                auto issueWindow = [&](uint32_t cb)
-                {
-                    uint32_t const ce = min(total, cb + uint32_t(CAP));
-                    if(lane == 0)
-                    {
-                        fenceProxyAsync();
-                        mbarExpectTx(bar, (ce - cb) * uint32_t(sizeof(V4)));
-                    }
-                    for(int sl = 0; sl < 27; ++sl)
-                    {
-                        uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
-                        uint32_t const n0 = __shfl_sync(0xffffffffu, sCnt, sl);
-                        uint32_t const b0 = __shfl_sync(0xffffffffu, sBeg, sl);
-                        if(p0 + n0 <= cb || p0 >= ce)
-                            continue;
-                        uint32_t const lo = max(p0, cb);
-                        uint32_t const hi2 = min(p0 + n0, ce);
-                        if(lane == 0)
-                            bulkCopyToShared(sRaw + (lo - cb), rec.pm + b0 + (lo - p0), (hi2 - lo) * uint32_t(sizeof(V4)), bar);
-                    }
-                };
-
                 // Two target chunks (up to 64 targets) share every staged window.
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
                 {
@@ -802,28 +708,10 @@ namespace sph
                     initChunk(A, rec, tc, tEnd, lane);
                     bool const twoChunks = tc + 32 < tEnd;
                     initChunk(Bc, rec, tc + 32, tEnd, lane);
-                    if constexpr(kBulk)
-                    {
-                        __syncwarp();
-                        issueWindow(0);
-                    }
                     for(uint32_t cb = 0; cb < total; cb += CAP)
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
                         __syncwarp();
-                        if constexpr(kBulk)
-                        {
-                            // warp-uniform decision: every lane leaves or none does
-                            if(!__all_sync(0xffffffffu, mbarWait(bar, phase)))
-                            {
-                                // give up: report, let the copies land (bounded), leave
-                                if(lane == 0)
-                                    atomicAdd(&c.status[kStatTimeout], 1u);
-                                mbarWait(bar, phase);
-                                return;
-                            }
-                            phase ^= 1u;
-                        }
                         for(int sl = 0; sl < 27; ++sl)
                         {
                             uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
@@ -839,11 +727,7 @@ namespace sph
                             for(uint32_t q = lo + uint32_t(lane); q < hi2; q += 32)
                             {
                                 uint32_t const j = b0 + (q - p0);
-                                V4 pj;
-                                if constexpr(kBulk)
-                                    pj = sRaw[q - cb];
-                                else
-                                    pj = ld4(rec.pm + j);
+                                V4 const pj = ld4(rec.pm + j);
                                 sNX[q - cb] = -addRn(pj.x, sx);
                                 sNY[q - cb] = -addRn(pj.y, sy);
                                 sNZ[q - cb] = -addRn(pj.z, sz);
@@ -851,13 +735,6 @@ namespace sph
                                 if constexpr(PAIRMAX)
                                     sH[q - cb] = rec.hc[j];
                             }
-                        }
-                        if constexpr(kBulk)
-                        {
-                            // sRaw is consumed: the next window's copies fly during the cull
-                            __syncwarp();
-                            if(cb + uint32_t(CAP) < total)
-                                issueWindow(cb + uint32_t(CAP));
                         }
                         uint32_t const m = ce - cb;
                         // far candidates up to the next multiple of 32
@@ -1158,10 +1035,7 @@ namespace sph
         template<typename T>
         constexpr size_t densitySmem()
         {
-            using V4 = typename PairCfg<T>::V4;
-            size_t const soa = size_t(kDensWarps) * PairCfg<T>::cap * (4 * sizeof(T) + sizeof(uint32_t));
-            // FP32 adds the raw bulk-copy window and one mbarrier per warp
-            return sizeof(T) == 4 ? soa + size_t(kDensWarps) * (PairCfg<T>::cap * sizeof(V4) + sizeof(uint64_t)) : soa;
+            return size_t(kDensWarps) * PairCfg<T>::cap * (4 * sizeof(T) + sizeof(uint32_t));
         }
 
         template<int K, typename T>

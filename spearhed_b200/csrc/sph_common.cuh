@@ -273,7 +273,6 @@ namespace sph
         kStatNonFinite = 2,  //!< non-finite positions
         kStatMaxCount = 3,   //!< largest neighbour count seen (list sizing)
         kStatBadInput = 4,   //!< gathered h / source masses that are not positive and finite
-        kStatTimeout = 5,    //!< warps whose bulk staging copies did not complete within the wait limit
         kStatWords = 8
     };
 } // namespace sph
