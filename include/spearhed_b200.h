@@ -246,6 +246,34 @@ int sph_set_clock(sph_ctx* ctx, int32_t nbox, const double* time, const double* 
  * replay it (on = 1) or launch the kernels one by one (on = 0, the default). */
 int sph_use_graph(sph_ctx* ctx, int32_t on);
 
+/* Launch shapes of the two pair kernels (no reference counterpart; the
+ * reference's frame size and threads per frame are compile-time constants,
+ * spmacc/Frame.hpp:49-132).  density: staging depth (candidates per shared-memory
+ * window) and register cap (blocks per SM); force: register cap. */
+typedef struct SphTuning
+{
+    int32_t density_variant;      /* index into the density shapes (0 = default)          */
+    int32_t force_variant;        /* index into the force shapes (0 = default)            */
+    int32_t staging_depth;        /* density candidates per shared-memory window          */
+    int32_t density_blocks_per_sm;
+    int32_t force_blocks_per_sm;
+    int32_t n_density_variants;   /* shapes available for this precision                 */
+    int32_t n_force_variants;
+    int32_t steps_per_trial;      /* steps timed per shape by sph_autotune (0: not tuned)  */
+    double density_ms[8];         /* per-step density time of each shape (sph_autotune)   */
+    double force_ms[8];           /* per-step force time of each shape (sph_autotune)     */
+} SphTuning;
+
+/* Times every launch shape of the density and force kernels on this context's
+ * current particles (steps_per_trial steps each, the state restored after every
+ * trial) and keeps the fastest of each.  The particles, clock and diagnostics are
+ * left as they were.  *out (may be NULL) receives the choice and the timings. */
+int sph_autotune(sph_ctx* ctx, int32_t steps_per_trial, SphTuning* out);
+
+/* Sets the launch shapes explicitly (e.g. the choice of an earlier sph_autotune). */
+int sph_set_tuning(sph_ctx* ctx, int32_t density_variant, int32_t force_variant);
+int sph_get_tuning(sph_ctx* ctx, SphTuning* out);
+
 /* Density summation that allocates no device memory, for callers that cannot
  * call cudaMalloc (no counterpart in the reference).
  *

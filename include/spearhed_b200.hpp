@@ -102,6 +102,13 @@ namespace spearhed_b200
             check(sph_reduce(ctx_, &d), "sph_reduce");
             return d;
         }
+        //! Picks the fastest launch shapes on the current particles (state kept).
+        SphTuning autotune(int32_t stepsPerTrial = 2)
+        {
+            SphTuning t{};
+            check(sph_autotune(ctx_, stepsPerTrial, &t), "sph_autotune");
+            return t;
+        }
 
     private:
         sph_ctx* ctx_ = nullptr;

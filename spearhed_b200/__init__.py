@@ -111,6 +111,21 @@ class Context:
     def use_graph(self, on: bool = True):
         abi.check(self._L.sph_use_graph(self._p, int(bool(on))))
 
+    def autotune(self, steps_per_trial: int = 2) -> dict:
+        """Times every launch shape of the pair kernels on the current particles
+        (the state is restored after each trial) and keeps the fastest."""
+        t = abi.SphTuning()
+        abi.check(self._L.sph_autotune(self._p, int(steps_per_trial), C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, density_variant: int, force_variant: int):
+        abi.check(self._L.sph_set_tuning(self._p, int(density_variant), int(force_variant)))
+
+    def tuning(self) -> dict:
+        t = abi.SphTuning()
+        abi.check(self._L.sph_get_tuning(self._p, C.byref(t)))
+        return t.as_dict()
+
     def close(self):
         if self._p:
             abi.check(self._L.sph_destroy(self._p))

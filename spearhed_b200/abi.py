@@ -183,6 +183,27 @@ class Species:
         return out
 
 
+class SphTuning(C.Structure):
+    _fields_ = [
+        ("density_variant", C.c_int32),
+        ("force_variant", C.c_int32),
+        ("staging_depth", C.c_int32),
+        ("density_blocks_per_sm", C.c_int32),
+        ("force_blocks_per_sm", C.c_int32),
+        ("n_density_variants", C.c_int32),
+        ("n_force_variants", C.c_int32),
+        ("steps_per_trial", C.c_int32),
+        ("density_ms", C.c_double * 8),
+        ("force_ms", C.c_double * 8),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_ms")}
+        d["density_ms"] = [self.density_ms[i] for i in range(self.n_density_variants)]
+        d["force_ms"] = [self.force_ms[i] for i in range(self.n_force_variants)]
+        return d
+
+
 _LIB = None
 
 
@@ -216,6 +237,9 @@ def lib():
         "sph_use_graph": (C.c_int, [ctx_p, C.c_int32]),
         "sph_get_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_set_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
+        "sph_autotune": (C.c_int, [ctx_p, C.c_int32, P(SphTuning)]),
+        "sph_set_tuning": (C.c_int, [ctx_p, C.c_int32, C.c_int32]),
+        "sph_get_tuning": (C.c_int, [ctx_p, P(SphTuning)]),
         "sph_last_error_string": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

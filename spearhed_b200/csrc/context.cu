@@ -179,6 +179,8 @@ struct sph_ctx
     double timings[5] = {0, 0, 0, 0, 0};
     // State a step call starts from, restored when a neighbour list overflowed
     // in any of its steps: the call then regrows the lists and runs again.
+    int densityVariant = 0, forceVariant = 0; //!< launch shapes (sph_autotune / sph_set_tuning)
+    SphTuning tuning{};
     bool haveSnap = false;
     sph::Master snap{};
     sph::BoxScalars snapBs{};
@@ -349,6 +351,8 @@ struct sph_ctx
     int checkStatus(char const* where);
     int snapshot(bool restore);
     int runSteps(int32_t nsteps);
+    int autotune(int32_t stepsPerTrial);
+    void describeTuning();
     int densityPass();
     int forcePass();
     int stepOnce(cudaEvent_t const* ev);
@@ -643,7 +647,7 @@ int sph_ctx::probeListCapacity()
         int st = clearStatus();
         if(st || (st = build(false)))
             return st;
-        sph::launchDensity(dc, pa, p.kernel, p.precision, true, stream);
+        sph::launchDensity(dc, pa, p.kernel, p.precision, true, densityVariant, stream);
         uint32_t stat[sph::kStatWords];
         SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost, stream));
         SPH_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -723,14 +727,14 @@ int sph_ctx::build(bool drift)
 int sph_ctx::densityPass()
 {
     SPH_CUDA_TRY(cudaMemsetAsync(dc.lists.count, 0xff, size_t(n) * 4, stream));
-    sph::launchDensity(dc, pa, p.kernel, p.precision, false, stream);
+    sph::launchDensity(dc, pa, p.kernel, p.precision, false, densityVariant, stream);
     return SPH_OK;
 }
 
 int sph_ctx::forcePass()
 {
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.dtBits, 0x7f, sizeof(unsigned long long) * dc.nbox, stream));
-    sph::launchForce(dc, pa, p.kernel, p.precision, stream);
+    sph::launchForce(dc, pa, p.kernel, p.precision, forceVariant, stream);
     return SPH_OK;
 }
 
@@ -865,6 +869,98 @@ int sph_ctx::steps(int32_t nsteps, double dt)
     densityValid = st == SPH_OK;
     forceValid = st == SPH_OK;
     return st;
+}
+
+//! Fills `tuning` with the current shapes.
+void sph_ctx::describeTuning()
+{
+    tuning.density_variant = densityVariant;
+    tuning.force_variant = forceVariant;
+    sph::densityShape(p.precision, densityVariant, &tuning.staging_depth, &tuning.density_blocks_per_sm);
+    tuning.force_blocks_per_sm = sph::forceBlocksPerSm(p.precision, int(p.physics), forceVariant);
+    tuning.n_density_variants = sph::densityVariants(p.precision);
+    tuning.n_force_variants = sph::forceVariants(p.precision);
+}
+
+//! Times every density and force launch shape over stepsPerTrial eager steps
+//! from the same saved state (restored after each trial, and at the end) and
+//! keeps the fastest of each.  Density and force shapes are independent, so
+//! each kernel's trials vary its own shape with the other at its default.
+int sph_ctx::autotune(int32_t stepsPerTrial)
+{
+    if(stepsPerTrial < 1)
+        return fail(SPH_ERR_INVALID, "sph_autotune: steps_per_trial must be >= 1");
+    int st = ensureDevice();
+    if(st || (st = snapshot(false)))
+        return st;
+    bool const graph = useGraph;
+    useGraph = false;
+    dropGraphs();
+    int const nd = sph::densityVariants(p.precision), nf = sph::forceVariants(p.precision);
+    tuning = SphTuning{};
+    for(int k = 0; k < 8; ++k)
+        tuning.density_ms[k] = tuning.force_ms[k] = 0.0;
+    int const d0 = densityVariant, f0 = forceVariant;
+    auto trial = [&](int dv, int fv, double& dms, double& fms) -> int
+    {
+        densityVariant = dv;
+        forceVariant = fv;
+        // one untimed step first (a kernel's first launch also loads its module)
+        int r = runSteps(1);
+        int const rs0 = snapshot(true);
+        if(rs0)
+            return rs0;
+        if(r != SPH_OK && r != SPH_ERR_OVERFLOW)
+            return r;
+        r = SPH_ERR_OVERFLOW;
+        for(int attempt = 0; attempt < 8 && r == SPH_ERR_OVERFLOW; ++attempt)
+        {
+            r = runSteps(stepsPerTrial);
+            if(r == SPH_ERR_OVERFLOW)
+            {
+                uint32_t stat[sph::kStatWords];
+                SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
+                int const g = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16);
+                if(g)
+                    return g;
+            }
+            int const rs = snapshot(true);
+            if(rs)
+                return rs;
+        }
+        dms = timings[1] / stepsPerTrial;
+        fms = timings[2] / stepsPerTrial;
+        return r;
+    };
+    double unused = 0.0;
+    int bestD = 0, bestF = 0;
+    for(int v = 0; v < nd && !st; ++v)
+    {
+        st = trial(v, 0, tuning.density_ms[v], unused);
+        if(!st && tuning.density_ms[v] < tuning.density_ms[bestD])
+            bestD = v;
+    }
+    for(int v = 0; v < nf && !st; ++v)
+    {
+        st = trial(0, v, unused, tuning.force_ms[v]);
+        if(!st && tuning.force_ms[v] < tuning.force_ms[bestF])
+            bestF = v;
+    }
+    useGraph = graph;
+    if(st)
+    {
+        densityVariant = d0;
+        forceVariant = f0;
+        return st;
+    }
+    densityVariant = bestD;
+    forceVariant = bestF;
+    // the particles are back where they were; the derivatives are a trial's
+    densityValid = false;
+    forceValid = false;
+    describeTuning();
+    tuning.steps_per_trial = stepsPerTrial;
+    return SPH_OK;
 }
 
 //! One attempt of a step call: the steps (pairs of them as CUDA graphs when
@@ -1391,6 +1487,45 @@ int sph_use_graph(sph_ctx* ctx, int32_t on)
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
     ctx->useGraph = on != 0;
+    return SPH_OK;
+}
+
+int sph_autotune(sph_ctx* ctx, int32_t steps_per_trial, SphTuning* out)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    int const st = ctx->autotune(steps_per_trial);
+    if(st)
+        return st;
+    if(out)
+        *out = ctx->tuning;
+    return SPH_OK;
+}
+
+int sph_set_tuning(sph_ctx* ctx, int32_t density_variant, int32_t force_variant)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    if(density_variant < 0 || density_variant >= sph::densityVariants(ctx->p.precision) || force_variant < 0
+       || force_variant >= sph::forceVariants(ctx->p.precision))
+        return fail(SPH_ERR_INVALID, "sph_set_tuning: no such launch shape for this precision");
+    if(ctx->densityVariant != density_variant || ctx->forceVariant != force_variant)
+        ctx->dropGraphs();
+    ctx->densityVariant = density_variant;
+    ctx->forceVariant = force_variant;
+    ctx->tuning.steps_per_trial = 0;
+    return SPH_OK;
+}
+
+int sph_get_tuning(sph_ctx* ctx, SphTuning* out)
+{
+    if(!ctx || !out)
+        return fail(SPH_ERR_INVALID, "sph_get_tuning: bad arguments");
+    int32_t const spt = ctx->tuning.steps_per_trial;
+    ctx->describeTuning();
+    *out = ctx->tuning;
+    out->steps_per_trial = spt;
     return SPH_OK;
 }
 

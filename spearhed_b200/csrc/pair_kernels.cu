@@ -31,13 +31,7 @@ namespace sph
     namespace
     {
         constexpr int kDensWarps = 4;
-#ifndef SPH_DENS_MIN_BLOCKS
-#define SPH_DENS_MIN_BLOCKS 6
-#endif
-        constexpr int kDensMinBlocks = SPH_DENS_MIN_BLOCKS; //!< FP32 density blocks per SM (register cap)
         constexpr int kForceThreads = 128;
-        constexpr int kForceMinBlocks = 5;    //!< FP32 hydro: caps registers near 100 per thread (20 warps per SM)
-        constexpr int kForceMinBlocksMhd = 4; //!< FP32 SPMHD: 128 registers, no spills (16 warps per SM)
         constexpr int kBlock = 8; //!< terms per compensated block
 
         template<typename T>
@@ -605,20 +599,23 @@ namespace sph
             return ft[2];
         }
 
-        template<int K, typename T, bool PAIRMAX>
-        __global__ void __launch_bounds__(kDensWarps * 32, sizeof(T) == 4 ? kDensMinBlocks : 4) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
+        //! Tunable launch shapes (picked per context by sph_autotune): CAP is the
+        //! staging depth (candidates per shared-memory window), MINB the blocks
+        //! per SM the register allocation must admit.
+        template<int K, typename T, bool PAIRMAX, int CAP, int MINB>
+        __global__ void __launch_bounds__(kDensWarps * 32, MINB) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
         {
             using V4 = typename PairCfg<T>::V4;
-            constexpr int CAP = PairCfg<T>::cap;
             extern __shared__ __align__(32) unsigned char smem[];
             int const warp = threadIdx.x >> 5;
             int const lane = threadIdx.x & 31;
-            // per warp: negated shifted x, y, z, smoothing length, list entry
+            // per warp: negated shifted x, y, z, (pair-max cull) smoothing length, list entry
+            constexpr int kCols = PAIRMAX ? 4 : 3;
             T* const sNX = reinterpret_cast<T*>(smem) + warp * CAP;
             T* const sNY = sNX + kDensWarps * CAP;
             T* const sNZ = sNY + kDensWarps * CAP;
-            T* const sH = sNZ + kDensWarps * CAP;
-            uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + 4 * kDensWarps * CAP)
+            T* const sH = sNZ + kDensWarps * CAP; // only with PAIRMAX
+            uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
                                    + warp * CAP;
             Records<V4, T> const rec = records<T>(c);
             T const supT = T(Kern<K>::support);
@@ -827,8 +824,8 @@ namespace sph
             }
         };
 
-        template<int K, typename T, int PH>
-        __global__ void __launch_bounds__(kForceThreads, sizeof(T) == 4 ? (PH >= 2 ? kForceMinBlocksMhd : kForceMinBlocks) : 3) kForce(DevCtx c, PhysArgs pa)
+        template<int K, typename T, int PH, int MINB>
+        __global__ void __launch_bounds__(kForceThreads, MINB) kForce(DevCtx c, PhysArgs pa)
         {
             using V4 = typename PairCfg<T>::V4;
             constexpr bool kMhd = PH >= 2;
@@ -1032,94 +1029,180 @@ namespace sph
                 atomicMin(&c.bs.dtBits[myBox], orderedBits(dtLocal));
         }
 
-        template<typename T>
+        template<typename T, bool PM, int CAP>
         constexpr size_t densitySmem()
         {
-            return size_t(kDensWarps) * PairCfg<T>::cap * (4 * sizeof(T) + sizeof(uint32_t));
+            return size_t(kDensWarps) * CAP * ((PM ? 4 : 3) * sizeof(T) + sizeof(uint32_t));
         }
 
-        template<int K, typename T>
-        void configureK()
+        // ---- launch-shape variants -------------------------------------------
+        // density FP32: (CAP, blocks/SM) = (256, 6), (256, 5), (128, 6), (128, 5);
+        // density FP64: (256, 4), (128, 4).  force FP32: blocks/SM 4 or 5 (SPMHD
+        // default 4, hydro default 5); force FP64: 3.  Variant 0 is the default.
+        constexpr int kDensVariants32 = 4, kDensVariants64 = 2, kForceVariants32 = 2, kForceVariants64 = 1;
+        constexpr int kDensCap32[kDensVariants32] = {256, 256, 128, 128};
+        constexpr int kDensBlk32[kDensVariants32] = {6, 5, 6, 5};
+        constexpr int kDensCap64[kDensVariants64] = {256, 128};
+
+        //! Shared-memory carve-out (percent of the maximum) that fits `blocks`
+        //! blocks of `smem` bytes; the rest of the unified array stays L1 for
+        //! the list gathers.
+        int carveout(size_t smem, int blocks)
         {
-            cudaFuncSetAttribute(kDensity<K, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(densitySmem<T>()));
-            cudaFuncSetAttribute(kDensity<K, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(densitySmem<T>()));
+            size_t const need = size_t(blocks) * (smem + 1024);
+            size_t const maxSmem = 228 * 1024;
+            int pct = int((need * 100 + maxSmem - 1) / maxSmem);
+            return pct > 100 ? 100 : pct;
         }
 
-        template<int K, typename T, bool PM>
-        void densityOne(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
+        template<int K, typename T, bool PM, int CAP, int MINB>
+        void configureDensity()
         {
-            size_t const smem = densitySmem<T>();
+            auto f = kDensity<K, T, PM, CAP, MINB>;
+            size_t const smem = densitySmem<T, PM, CAP>();
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carveout(smem, MINB));
+        }
+
+        template<int K, typename T, int PH, int MINB>
+        void configureForce()
+        {
+            cudaFuncSetAttribute(kForce<K, T, PH, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        }
+
+        template<int K, typename T, bool PM, int CAP, int MINB>
+        void densityLaunch(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
+        {
+            size_t const smem = densitySmem<T, PM, CAP>();
             // persistent grid: enough resident blocks to fill every SM; cells come
             // from the work queue
             uint32_t blocks = (c.cells.ncells + kDensWarps - 1) / kDensWarps;
-            uint32_t const resident = 148u * (sizeof(T) == 4 ? kDensMinBlocks : 4);
+            uint32_t const resident = 148u * uint32_t(MINB);
             blocks = blocks > resident ? resident : blocks;
             if(blocks)
             {
                 cudaMemsetAsync(c.work, 0, sizeof(uint32_t), s);
-                kDensity<K, T, PM><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
+                kDensity<K, T, PM, CAP, MINB><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
                 countLaunches(1);
             }
         }
 
-        template<int K, typename T>
-        void densityPM(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
+        template<int K, typename T, bool PM>
+        void densityOne(DevCtx const& c, PhysArgs const& pa, bool countOnly, int variant, cudaStream_t s)
         {
-            if(pa.cull == SPH_CULL_PAIR_MAX)
-                densityOne<K, T, true>(c, pa, countOnly, s);
+            if constexpr(sizeof(T) == 4)
+            {
+                switch(variant)
+                {
+                case 1: densityLaunch<K, T, PM, kDensCap32[1], kDensBlk32[1]>(c, pa, countOnly, s); break;
+                case 2: densityLaunch<K, T, PM, kDensCap32[2], kDensBlk32[2]>(c, pa, countOnly, s); break;
+                case 3: densityLaunch<K, T, PM, kDensCap32[3], kDensBlk32[3]>(c, pa, countOnly, s); break;
+                default: densityLaunch<K, T, PM, kDensCap32[0], kDensBlk32[0]>(c, pa, countOnly, s); break;
+                }
+            }
             else
-                densityOne<K, T, false>(c, pa, countOnly, s);
+            {
+                if(variant == 1)
+                    densityLaunch<K, T, PM, kDensCap64[1], 4>(c, pa, countOnly, s);
+                else
+                    densityLaunch<K, T, PM, kDensCap64[0], 4>(c, pa, countOnly, s);
+            }
         }
 
         template<int K, typename T>
-        void forceOne(DevCtx const& c, PhysArgs const& pa, cudaStream_t s)
+        void densityPM(DevCtx const& c, PhysArgs const& pa, bool countOnly, int variant, cudaStream_t s)
+        {
+            if(pa.cull == SPH_CULL_PAIR_MAX)
+                densityOne<K, T, true>(c, pa, countOnly, variant, s);
+            else
+                densityOne<K, T, false>(c, pa, countOnly, variant, s);
+        }
+
+        template<int K, typename T, int PH>
+        void forceLaunch(DevCtx const& c, PhysArgs const& pa, int variant, cudaStream_t s)
         {
             unsigned const g = (c.n + kForceThreads - 1) / kForceThreads;
             if(!g)
                 return;
+            if constexpr(sizeof(T) == 4)
+            {
+                // variant 0: SPMHD 4 blocks/SM (128 registers), hydro 5; variant 1 the other
+                constexpr int a = PH >= 2 ? 4 : 5, b = PH >= 2 ? 5 : 4;
+                if(variant == 1)
+                    kForce<K, T, PH, b><<<g, kForceThreads, 0, s>>>(c, pa);
+                else
+                    kForce<K, T, PH, a><<<g, kForceThreads, 0, s>>>(c, pa);
+            }
+            else
+                kForce<K, T, PH, 3><<<g, kForceThreads, 0, s>>>(c, pa);
+            countLaunches(1);
+        }
+
+        template<int K, typename T>
+        void forceOne(DevCtx const& c, PhysArgs const& pa, int variant, cudaStream_t s)
+        {
             uint32_t const full = SPH_PHYS_MHD | SPH_PHYS_AV | SPH_PHYS_DEDNER | SPH_PHYS_TENSILE;
             if((pa.physics & full) == full)
-            {
-                kForce<K, T, 3><<<g, kForceThreads, 0, s>>>(c, pa);
-                countLaunches(1);
-            }
+                forceLaunch<K, T, 3>(c, pa, variant, s);
             else if(pa.physics & SPH_PHYS_MHD)
-            {
-                kForce<K, T, 2><<<g, kForceThreads, 0, s>>>(c, pa);
-                countLaunches(1);
-            }
+                forceLaunch<K, T, 2>(c, pa, variant, s);
             else if(pa.physics & SPH_PHYS_AV)
-            {
-                kForce<K, T, 1><<<g, kForceThreads, 0, s>>>(c, pa);
-                countLaunches(1);
-            }
+                forceLaunch<K, T, 1>(c, pa, variant, s);
             else
-            {
-                kForce<K, T, 0><<<g, kForceThreads, 0, s>>>(c, pa);
-                countLaunches(1);
-            }
+                forceLaunch<K, T, 0>(c, pa, variant, s);
         }
 
         template<typename T>
-        void densityK(DevCtx const& c, PhysArgs const& pa, int kernel, bool countOnly, cudaStream_t s)
+        void densityK(DevCtx const& c, PhysArgs const& pa, int kernel, bool countOnly, int variant, cudaStream_t s)
         {
             if(kernel == SPH_KERNEL_QUINTIC)
-                densityPM<SPH_KERNEL_QUINTIC, T>(c, pa, countOnly, s);
+                densityPM<SPH_KERNEL_QUINTIC, T>(c, pa, countOnly, variant, s);
             else if(kernel == SPH_KERNEL_WENDLAND_C2)
-                densityPM<SPH_KERNEL_WENDLAND_C2, T>(c, pa, countOnly, s);
+                densityPM<SPH_KERNEL_WENDLAND_C2, T>(c, pa, countOnly, variant, s);
             else
-                densityPM<SPH_KERNEL_CUBIC, T>(c, pa, countOnly, s);
+                densityPM<SPH_KERNEL_CUBIC, T>(c, pa, countOnly, variant, s);
         }
 
         template<typename T>
-        void forceK(DevCtx const& c, PhysArgs const& pa, int kernel, cudaStream_t s)
+        void forceK(DevCtx const& c, PhysArgs const& pa, int kernel, int variant, cudaStream_t s)
         {
             if(kernel == SPH_KERNEL_QUINTIC)
-                forceOne<SPH_KERNEL_QUINTIC, T>(c, pa, s);
+                forceOne<SPH_KERNEL_QUINTIC, T>(c, pa, variant, s);
             else if(kernel == SPH_KERNEL_WENDLAND_C2)
-                forceOne<SPH_KERNEL_WENDLAND_C2, T>(c, pa, s);
+                forceOne<SPH_KERNEL_WENDLAND_C2, T>(c, pa, variant, s);
             else
-                forceOne<SPH_KERNEL_CUBIC, T>(c, pa, s);
+                forceOne<SPH_KERNEL_CUBIC, T>(c, pa, variant, s);
+        }
+
+        template<int K, bool PM>
+        void configureDensityK()
+        {
+            configureDensity<K, float, PM, kDensCap32[0], kDensBlk32[0]>();
+            configureDensity<K, float, PM, kDensCap32[1], kDensBlk32[1]>();
+            configureDensity<K, float, PM, kDensCap32[2], kDensBlk32[2]>();
+            configureDensity<K, float, PM, kDensCap32[3], kDensBlk32[3]>();
+            configureDensity<K, double, PM, kDensCap64[0], 4>();
+            configureDensity<K, double, PM, kDensCap64[1], 4>();
+        }
+
+        template<int K, int PH>
+        void configureForceK()
+        {
+            constexpr int a = PH >= 2 ? 4 : 5, b = PH >= 2 ? 5 : 4;
+            configureForce<K, float, PH, a>();
+            configureForce<K, float, PH, b>();
+            configureForce<K, double, PH, 3>();
+        }
+
+        template<int K>
+        void configureK()
+        {
+            configureDensityK<K, true>();
+            configureDensityK<K, false>();
+            configureForceK<K, 0>();
+            configureForceK<K, 1>();
+            configureForceK<K, 2>();
+            configureForceK<K, 3>();
         }
     } // namespace
 
@@ -1128,28 +1211,58 @@ namespace sph
         static bool done = false;
         if(done)
             return;
-        configureK<SPH_KERNEL_CUBIC, float>();
-        configureK<SPH_KERNEL_QUINTIC, float>();
-        configureK<SPH_KERNEL_WENDLAND_C2, float>();
-        configureK<SPH_KERNEL_CUBIC, double>();
-        configureK<SPH_KERNEL_QUINTIC, double>();
-        configureK<SPH_KERNEL_WENDLAND_C2, double>();
+        configureK<SPH_KERNEL_CUBIC>();
+        configureK<SPH_KERNEL_QUINTIC>();
+        configureK<SPH_KERNEL_WENDLAND_C2>();
         done = true;
     }
 
-    void launchDensity(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, bool countOnly, cudaStream_t s)
+    int densityVariants(int precision)
     {
-        if(precision == SPH_PREC_FP64)
-            densityK<double>(c, pa, kernel, countOnly, s);
-        else
-            densityK<float>(c, pa, kernel, countOnly, s);
+        return precision == SPH_PREC_FP64 ? kDensVariants64 : kDensVariants32;
     }
 
-    void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, cudaStream_t s)
+    int forceVariants(int precision)
+    {
+        return precision == SPH_PREC_FP64 ? kForceVariants64 : kForceVariants32;
+    }
+
+    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm)
+    {
+        bool const f64 = precision == SPH_PREC_FP64;
+        int const v = variant < 0 || variant >= densityVariants(precision) ? 0 : variant;
+        *stagingDepth = f64 ? kDensCap64[v] : kDensCap32[v];
+        *blocksPerSm = f64 ? 4 : kDensBlk32[v];
+    }
+
+    int forceBlocksPerSm(int precision, int physics, int variant)
     {
         if(precision == SPH_PREC_FP64)
-            forceK<double>(c, pa, kernel, s);
+            return 3;
+        bool const mhd = physics & SPH_PHYS_MHD;
+        return (variant == 1) == mhd ? 5 : 4;
+    }
+
+    void launchDensity(
+        DevCtx const& c,
+        PhysArgs const& pa,
+        int kernel,
+        int precision,
+        bool countOnly,
+        int variant,
+        cudaStream_t s)
+    {
+        if(precision == SPH_PREC_FP64)
+            densityK<double>(c, pa, kernel, countOnly, variant, s);
         else
-            forceK<float>(c, pa, kernel, s);
+            densityK<float>(c, pa, kernel, countOnly, variant, s);
+    }
+
+    void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, int variant, cudaStream_t s)
+    {
+        if(precision == SPH_PREC_FP64)
+            forceK<double>(c, pa, kernel, variant, s);
+        else
+            forceK<float>(c, pa, kernel, variant, s);
     }
 } // namespace sph

@@ -262,8 +262,21 @@ namespace sph
 
     // ---- pair_kernels.cu
     //! Neighbour build + density (+ records for the force pass); countOnly only counts.
-    void launchDensity(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, bool countOnly, cudaStream_t s);
-    void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, cudaStream_t s);
+    //! Pair-kernel launches; `variant` picks the launch shape (0 = default,
+    //! see densityVariants / forceVariants).
+    void launchDensity(
+        DevCtx const& c,
+        PhysArgs const& pa,
+        int kernel,
+        int precision,
+        bool countOnly,
+        int variant,
+        cudaStream_t s);
+    void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, int variant, cudaStream_t s);
+    int densityVariants(int precision);
+    int forceVariants(int precision);
+    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm);
+    int forceBlocksPerSm(int precision, int physics, int variant);
     //! Sets the shared-memory attributes of every pair-kernel instantiation
     //! (once, before any launch, so no attribute call happens during a graph capture).
     void configurePairKernels();
