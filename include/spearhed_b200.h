@@ -249,7 +249,8 @@ int sph_use_graph(sph_ctx* ctx, int32_t on);
 /* Launch shapes of the two pair kernels (no reference counterpart; the
  * reference's frame size and threads per frame are compile-time constants,
  * spmacc/Frame.hpp:49-132).  density: staging depth (candidates per shared-memory
- * window) and register cap (blocks per SM); force: register cap. */
+ * window) and register cap (blocks per SM); force: register cap.  Every shape
+ * gives identical bits. */
 typedef struct SphTuning
 {
     int32_t density_variant;      /* index into the density shapes (0 = default)          */

@@ -824,6 +824,187 @@ namespace sph
             }
         };
 
+        //! Target-side data of the force pass.
+        template<typename V4, typename T>
+        struct OwnTarget
+        {
+            V4 pi, vi, ti, bi;
+            HConst<T> hk;
+            T alpha, beta, eps, rho2i;
+            bool av, dedner, tensile;
+        };
+
+        template<int K, typename T, int PH, typename V4>
+        __device__ __forceinline__ OwnTarget<V4, T> loadOwn(
+            Records<V4, T> const& rec,
+            PhysArgs const& pa,
+            uint32_t t)
+        {
+            OwnTarget<V4, T> o;
+            o.av = (PH == 1) || (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
+            o.dedner = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_DEDNER));
+            o.tensile = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_TENSILE));
+            o.pi = ld4(rec.pm + t);
+            o.vi = ld4(rec.fv + t);
+            o.ti = ld4(rec.ft + t);
+            o.bi = V4{};
+            if constexpr(PH >= 2)
+                o.bi = ld4(rec.fb + t);
+            o.hk = hconst<K, T>(o.vi.w);
+            o.alpha = T(pa.alpha);
+            o.beta = T(pa.beta);
+            o.eps = T(pa.avEps);
+            o.rho2i = o.ti.x * o.ti.x;
+            return o;
+        }
+
+        //! One pair term of the force pass: source records pj, vj, tj, bj and
+        //! the source's stencil image shift sh.
+        template<int K, typename T, int PH, typename V4>
+        __device__ __forceinline__ void pairTerm(
+            OwnTarget<V4, T> const& ow,
+            ForceAcc<V4, T>& A,
+            V4 const& pj,
+            V4 const& vj,
+            V4 const& tj,
+            V4 const& bj,
+            V4 const& sh)
+        {
+            V4 const& pi = ow.pi;
+            V4 const& vi = ow.vi;
+            V4 const& ti = ow.ti;
+            V4 const& bi = ow.bi;
+            T const rx = pi.x - (pj.x + sh.x);
+            T const ry = pi.y - (pj.y + sh.y);
+            T const rz = pi.z - (pj.z + sh.z);
+            T const r2 = rx * rx + ry * ry + rz * rz;
+            T const y = rsqrtT(r2);
+            T const invR = r2 > T(0) ? y : T(0);
+            T const r = r2 * invR;
+            T const si = gradWScalar<K, T>(r, invR, ow.hk);
+            T sj = si; // equal smoothing lengths give the same factor
+            if(vj.w != vi.w)
+                sj = gradWScalar<K, T>(r, invR, hconstFromInv<K, T>(rcpT(vj.w)));
+            T const mj = pj.w;
+            T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+            T const vr = vx * rx + vy * ry + vz * rz;
+            T const msi = mj * si;
+            // Isotropic pressure gradient (HydroForces.hpp:155-166).
+            T f = -mj * (ti.y * si + tj.y * sj);
+            if(ow.av)
+            {
+                // branch-free: mu = 0 (no viscosity) for receding pairs
+                T const vn = vr < T(0) ? vr : T(0);
+                T const hb = T(0.5) * (vi.w + vj.w);
+                T const mu = divT(hb * vn, r2 + ow.eps * hb * hb);
+                T const cb = T(0.5) * (ti.z + tj.z);
+                T const rb = T(0.5) * (ti.x + tj.x);
+                T const Pi = divT(-ow.alpha * cb * mu + ow.beta * mu * mu, rb);
+                T const g = mj * Pi * T(0.5) * (si + sj);
+                f -= g;
+                A.duav.add(T(0.5) * g * vr);
+            }
+            T fx = f * rx, fy = f * ry, fz = f * rz;
+            A.D.add(msi * vr);
+            T const w = vr * invR;
+            T const vs = ti.z + tj.z - ow.beta * (w < T(0) ? w : T(0));
+            A.vsig = vs > A.vsig ? vs : A.vsig;
+            if constexpr(PH >= 2)
+            {
+                T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
+                T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
+                T const cj = mj * sj * Bjr * tj.w;
+                if(ow.tensile)
+                {
+                    // stress + Borve: c_i B_i + c_j B_j - B_i (c_i + c_j) = c_j (B_j - B_i)
+                    fx += cj * (bj.x - bi.x);
+                    fy += cj * (bj.y - bi.y);
+                    fz += cj * (bj.z - bi.z);
+                }
+                else
+                {
+                    T const ci = msi * Bir * ti.w;
+                    fx += ci * bi.x + cj * bj.x;
+                    fy += ci * bi.y + cj * bj.y;
+                    fz += ci * bi.z + cj * bj.z;
+                }
+                T const wB = msi * Bir;
+                T gx = wB * vx, gy = wB * vy, gz = wB * vz;
+                if(ow.dedner)
+                {
+                    // rho_i^2 * m_j (psi_i/rho_i^2 s_i + psi_j/rho_j^2 s_j) r
+                    T const g = ow.rho2i * mj * (bi.w * si + bj.w * sj);
+                    gx += g * rx;
+                    gy += g * ry;
+                    gz += g * rz;
+                }
+                A.tx.add(gx);
+                A.ty.add(gy);
+                A.tz.add(gz);
+                A.divb.add(msi * (Bir - Bjr));
+            }
+            A.ax.add(fx);
+            A.ay.add(fy);
+            A.az.add(fz);
+        }
+
+        //! FP64 epilogue of one target: derivatives and its CFL time step.
+        template<typename T, int PH, typename V4>
+        __device__ __forceinline__ double forceEpilogue(
+            DevCtx const& c,
+            PhysArgs const& pa,
+            uint32_t t,
+            int box,
+            ForceAcc<V4, T> const& A,
+            bool dedner)
+        {
+            double const rho = c.cur.rho[t];
+            double const h = c.cur.h[t];
+            double const pr2 = (pa.gamma - 1.0) * c.cur.u[t] / rho; // P_i / rho_i^2
+            double const a[3] = {A.ax.value(), A.ay.value(), A.az.value()};
+            double const Dv = A.D.value();
+            c.d.dudt[t] = pr2 * Dv + A.duav.value();
+            if constexpr(PH >= 2)
+            {
+                double const Bi[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
+                double const psi = c.cur.psi[t];
+                double const tv[3] = {A.tx.value(), A.ty.value(), A.tz.value()};
+                double const invRho = 1.0 / rho;
+                double const divB = -invRho * A.divb.value();
+                double const divv = -invRho * Dv;
+                double const ch = __longlong_as_double(static_cast<long long>(c.bs.chBits[box]));
+                // dB/dt = -(1/rho)(T_induction - B_i D) - rho grad(psi); T carries rho^2 grad(psi)/rho.
+#pragma unroll
+                for(int q = 0; q < 3; ++q)
+                    c.d.dBdt[q][t] = -invRho * (tv[q] - Bi[q] * Dv);
+                c.d.divB[t] = divB;
+                c.d.dpsidt[t] = dedner ? (-ch * ch * divB - psi * pa.sigma * ch / h - 0.5 * psi * divv) : 0.0;
+            }
+#pragma unroll
+            for(int q = 0; q < 3; ++q)
+                c.d.dvdt[q][t] = a[q];
+            double dt = pa.cfl * h / double(A.vsig);
+            double const amag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+            if(amag > 0.0 && pa.cflForce > 0.0)
+                dt = fmin(dt, pa.cflForce * sqrt(h / amag));
+            return dt;
+        }
+
+        //! Physics variants compiled separately: 0 = the reference's inviscid
+        //! hydro, 1 = hydro + viscosity, 2 = SPMHD with viscosity, Dedner and the
+        //! tensile correction switched at run time, 3 = SPMHD with all three on.
+        //!
+        //! Accumulators (compensated in FP32): a (pressure, viscosity and magnetic
+        //! force together), D = sum m_j s_i v_ij.r (P dV work, div v and the
+        //! induction's B_i term), the viscous heating, T = sum m_j s_i (B_i.r) v_ij
+        //! + rho_i^2 (Dedner gradient term) for the induction, and the div B sum.
+        //! With the tensile correction the Maxwell-stress force and the Borve term
+        //! combine to sum m_j s_j (B_j.r)/(mu0 rho_j^2) (B_j - B_i).
+        //!
+        //! kForce: one thread per target.  The row is read 16 bytes (four
+        //! entries) at a time; the records of the next entry are in flight while
+        //! the current one is used.  Entries run in row order and the compensated
+        //! blocks hold 8 terms, as in the density pass.
         template<int K, typename T, int PH, int MINB>
         __global__ void __launch_bounds__(kForceThreads, MINB) kForce(DevCtx c, PhysArgs pa)
         {
@@ -836,99 +1017,10 @@ namespace sph
             int const myBox = t < c.n ? c.cur.box[t] : -1;
             if(act)
             {
-                bool const av = (PH == 1) || (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_AV));
-                bool const dedner = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_DEDNER));
-                bool const tensile = (PH == 3) || (PH == 2 && (pa.physics & SPH_PHYS_TENSILE));
+                OwnTarget<V4, T> const own = loadOwn<K, T, PH>(rec, pa, t);
                 V4 const* const stab = shiftTable<T>(c, myBox);
-                V4 const pi = ld4(rec.pm + t);
-                V4 const vi = ld4(rec.fv + t);
-                V4 const ti = ld4(rec.ft + t);
-                V4 bi{};
-                if constexpr(kMhd)
-                    bi = ld4(rec.fb + t);
-                HConst<T> const hk = hconst<K, T>(vi.w);
-                T const alpha = T(pa.alpha), beta = T(pa.beta), eps = T(pa.avEps);
-                T const rho2i = ti.x * ti.x;
                 ForceAcc<V4, T> A;
-                A.vsig = ti.z;
-
-                // one pair term, records of source j and its image shift o
-                auto pair = [&](V4 const& pj, V4 const& vj, V4 const& tj, V4 const& bj, V4 const& o)
-                {
-                    T const rx = pi.x - (pj.x + o.x);
-                    T const ry = pi.y - (pj.y + o.y);
-                    T const rz = pi.z - (pj.z + o.z);
-                    T const r2 = rx * rx + ry * ry + rz * rz;
-                    T const y = rsqrtT(r2);
-                    T const invR = r2 > T(0) ? y : T(0);
-                    T const r = r2 * invR;
-                    T const si = gradWScalar<K, T>(r, invR, hk);
-                    T sj = si; // equal smoothing lengths give the same factor
-                    if(vj.w != vi.w)
-                        sj = gradWScalar<K, T>(r, invR, hconstFromInv<K, T>(rcpT(vj.w)));
-                    T const mj = pj.w;
-                    T const vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-                    T const vr = vx * rx + vy * ry + vz * rz;
-                    T const msi = mj * si;
-                    // Isotropic pressure gradient (HydroForces.hpp:155-166).
-                    T f = -mj * (ti.y * si + tj.y * sj);
-                    if(av)
-                    {
-                        // branch-free: mu = 0 (no viscosity) for receding pairs
-                        T const vn = vr < T(0) ? vr : T(0);
-                        T const hb = T(0.5) * (vi.w + vj.w);
-                        T const mu = divT(hb * vn, r2 + eps * hb * hb);
-                        T const cb = T(0.5) * (ti.z + tj.z);
-                        T const rb = T(0.5) * (ti.x + tj.x);
-                        T const Pi = divT(-alpha * cb * mu + beta * mu * mu, rb);
-                        T const g = mj * Pi * T(0.5) * (si + sj);
-                        f -= g;
-                        A.duav.add(T(0.5) * g * vr);
-                    }
-                    T fx = f * rx, fy = f * ry, fz = f * rz;
-                    A.D.add(msi * vr);
-                    T const w = vr * invR;
-                    T const vs = ti.z + tj.z - beta * (w < T(0) ? w : T(0));
-                    A.vsig = vs > A.vsig ? vs : A.vsig;
-                    if constexpr(kMhd)
-                    {
-                        T const Bir = bi.x * rx + bi.y * ry + bi.z * rz;
-                        T const Bjr = bj.x * rx + bj.y * ry + bj.z * rz;
-                        T const cj = mj * sj * Bjr * tj.w;
-                        if(tensile)
-                        {
-                            // stress + Borve: c_i B_i + c_j B_j - B_i (c_i + c_j) = c_j (B_j - B_i)
-                            fx += cj * (bj.x - bi.x);
-                            fy += cj * (bj.y - bi.y);
-                            fz += cj * (bj.z - bi.z);
-                        }
-                        else
-                        {
-                            T const ci = msi * Bir * ti.w;
-                            fx += ci * bi.x + cj * bj.x;
-                            fy += ci * bi.y + cj * bj.y;
-                            fz += ci * bi.z + cj * bj.z;
-                        }
-                        T const wB = msi * Bir;
-                        T gx = wB * vx, gy = wB * vy, gz = wB * vz;
-                        if(dedner)
-                        {
-                            // rho_i^2 * m_j (psi_i/rho_i^2 s_i + psi_j/rho_j^2 s_j) r
-                            T const g = rho2i * mj * (bi.w * si + bj.w * sj);
-                            gx += g * rx;
-                            gy += g * ry;
-                            gz += g * rz;
-                        }
-                        A.tx.add(gx);
-                        A.ty.add(gy);
-                        A.tz.add(gz);
-                        A.divb.add(msi * (Bir - Bjr));
-                    }
-                    A.ax.add(fx);
-                    A.ay.add(fy);
-                    A.az.add(fz);
-                };
-
+                A.vsig = own.ti.z;
                 uint32_t const n = min(c.lists.count[t], c.lists.cap);
                 // rows are 32-byte aligned and hold a multiple of 8 entries
                 uint4 const* row4 = reinterpret_cast<uint4 const*>(c.lists.list + size_t(t) * c.lists.cap);
@@ -950,7 +1042,7 @@ namespace sph
                     V4 const pj = npm, vj = nfv, tj = nft, bj = nfb;
                     V4 const o = ld4(stab + nslot);
                     fetch(next);
-                    pair(pj, vj, tj, bj, o);
+                    pairTerm<K, T, PH>(own, A, pj, vj, tj, bj, o);
                 };
                 uint4 qc = make_uint4(0, 0, 0, 0);
                 if(n > 0)
@@ -984,38 +1076,7 @@ namespace sph
                         step(qc.z);
                 }
                 A.fold();
-
-                // Epilogue in FP64.
-                double const rho = c.cur.rho[t];
-                double const h = c.cur.h[t];
-                double const pr2 = (pa.gamma - 1.0) * c.cur.u[t] / rho; // P_i / rho_i^2
-                double const a[3] = {A.ax.value(), A.ay.value(), A.az.value()};
-                double const Dv = A.D.value();
-                c.d.dudt[t] = pr2 * Dv + A.duav.value();
-                if constexpr(kMhd)
-                {
-                    double const Bi[3] = {c.cur.B[0][t], c.cur.B[1][t], c.cur.B[2][t]};
-                    double const psi = c.cur.psi[t];
-                    double const tv[3] = {A.tx.value(), A.ty.value(), A.tz.value()};
-                    double const invRho = 1.0 / rho;
-                    double const divB = -invRho * A.divb.value();
-                    double const divv = -invRho * Dv;
-                    double const ch = __longlong_as_double(static_cast<long long>(c.bs.chBits[myBox]));
-                    // dB/dt = -(1/rho)(T_induction - B_i D) - rho grad(psi); T carries rho^2 grad(psi)/rho.
-#pragma unroll
-                    for(int q = 0; q < 3; ++q)
-                        c.d.dBdt[q][t] = -invRho * (tv[q] - Bi[q] * Dv);
-                    c.d.divB[t] = divB;
-                    c.d.dpsidt[t] = dedner ? (-ch * ch * divB - psi * pa.sigma * ch / h - 0.5 * psi * divv) : 0.0;
-                }
-#pragma unroll
-                for(int q = 0; q < 3; ++q)
-                    c.d.dvdt[q][t] = a[q];
-                double dt = pa.cfl * h / double(A.vsig);
-                double const amag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
-                if(amag > 0.0 && pa.cflForce > 0.0)
-                    dt = fmin(dt, pa.cflForce * sqrt(h / amag));
-                dtLocal = dt;
+                dtLocal = forceEpilogue<T, PH>(c, pa, t, myBox, A, own.dedner);
             }
             // CFL minimum per box: one atomic per warp when the warp is in one box
             int const box0 = __shfl_sync(0xffffffffu, myBox, 0);
@@ -1037,7 +1098,7 @@ namespace sph
 
         // ---- launch-shape variants -------------------------------------------
         // density FP32: (CAP, blocks/SM) = (256, 6), (256, 5), (128, 6), (128, 5);
-        // density FP64: (256, 4), (128, 4).  force FP32: blocks/SM 4 or 5 (SPMHD
+        // density FP64: (256, 4), (128, 4).  force FP32: 4 or 5 blocks/SM (SPMHD
         // default 4, hydro default 5); force FP64: 3.  Variant 0 is the default.
         constexpr int kDensVariants32 = 4, kDensVariants64 = 2, kForceVariants32 = 2, kForceVariants64 = 1;
         constexpr int kDensCap32[kDensVariants32] = {256, 256, 128, 128};
@@ -1242,6 +1303,7 @@ namespace sph
         bool const mhd = physics & SPH_PHYS_MHD;
         return (variant == 1) == mhd ? 5 : 4;
     }
+
 
     void launchDensity(
         DevCtx const& c,
