@@ -853,7 +853,16 @@ int sph_ctx::steps(int32_t nsteps, double dt)
     for(int attempt = 0;; ++attempt)
     {
         st = runSteps(nsteps);
-        if(st != SPH_ERR_OVERFLOW || attempt == kMaxReplays)
+        if(st == SPH_ERR_OVERFLOW && attempt == kMaxReplays)
+        {
+            // give up with the state the call started from
+            int const rs = snapshot(true);
+            if(rs)
+                return rs;
+            SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+            break;
+        }
+        if(st != SPH_ERR_OVERFLOW)
             break;
         uint32_t stat[sph::kStatWords];
         SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
