@@ -275,6 +275,64 @@ int sph_autotune(sph_ctx* ctx, int32_t steps_per_trial, SphTuning* out);
 int sph_set_tuning(sph_ctx* ctx, int32_t density_variant, int32_t force_variant);
 int sph_get_tuning(sph_ctx* ctx, SphTuning* out);
 
+/* ---- Device initialiser of particle species from lattice blocks ----
+ * Replaces: the setup blocks (regions per species with a count and a placement
+ * recipe, include/spearhed/particles/initialization/SetupInterface.hpp:34-113),
+ * the init driver that counts, scans and places them on the device
+ * (InitParticles.hpp:284-433) and simple-cubic placement at cell centres
+ * (spmacc/particles/initialization/SC.hpp:118-200).  A block is a region filled by
+ * an SC lattice, with constant state; a profile adds the analytic fields of the
+ * validation setups after an optional per-group jitter and periodic wrap. */
+enum
+{
+    SPH_MASK_NONE = 0,
+    SPH_MASK_INSIDE_DISC_XY = 1,  /* keep sites with hypot(x - cx, y - cy) <  radius */
+    SPH_MASK_OUTSIDE_DISC_XY = 2  /* keep sites with hypot(x - cx, y - cy) >= radius */
+};
+enum
+{
+    SPH_PROFILE_CONSTANT = 0,
+    SPH_PROFILE_ORSZAG_TANG = 1,       /* v = (-sin 2pi y, sin 2pi x, 0), B = p0 (-sin 2pi y, sin 4pi x, 0) */
+    SPH_PROFILE_KH_PERTURBATION = 2,   /* v_y = p0 sin(4 pi x) */
+    SPH_PROFILE_ROTOR = 3              /* rotation p2 about (p0, p1) for r < p3, times clip((p4 - r) / p5, 0, 1) beyond */
+};
+
+typedef struct SphLatticeBlock
+{
+    double lo[3], hi[3];       /* region volume                                                   */
+    int32_t counts[3];         /* lattice sites per axis; all 0: from spacing (sph_sc_cell_counts) */
+    int32_t mask;              /* SPH_MASK_*                                                      */
+    double spacing;
+    double mask_centre[2];
+    double mask_radius;
+    int32_t box_id;
+    int32_t jitter_group;      /* consecutive blocks with one id share one jitter stream           */
+    double jitter;             /* the group's uniform displacement amplitude per axis (length)     */
+    uint64_t seed;             /* the group's Philox4x64-10 key                                    */
+    double mass, h, density, u, psi;
+    double vel[3], B[3];
+} SphLatticeBlock;
+
+typedef struct SphInitProfile
+{
+    int32_t kind;              /* SPH_PROFILE_*                                                   */
+    int32_t wrap[3];           /* wrap positions periodically into [wrap_lo, wrap_hi) per axis    */
+    double wrap_lo[3], wrap_hi[3];
+    double p[8];               /* profile parameters                                              */
+} SphInitProfile;
+
+/* Generates the species on the device from nblocks lattice blocks (kept sites in
+ * block order, each block's sites x-fastest) and sets it as sph_set_species would;
+ * *n_out (may be NULL) receives the particle count.  profile may be NULL. */
+int sph_init_lattice(sph_ctx* ctx, int32_t species_id, uint32_t roles, int32_t nblocks,
+                     const SphLatticeBlock* blocks, const SphInitProfile* profile, int64_t* n_out);
+
+/* Replaces: computeSCCellCounts (spmacc/particles/initialization/SC.hpp:98-132):
+ * SC sites per axis of the box lo..hi at `spacing` (axis 0 truncated with a
+ * round-off snap, transverse axes rounded, each at least 1), in double or float. */
+int sph_sc_cell_counts(const double* lo, const double* hi, double spacing, uint32_t* counts);
+int sph_sc_cell_counts_f32(const float* lo, const float* hi, float spacing, uint32_t* counts);
+
 /* Density summation that allocates no device memory, for callers that cannot
  * call cudaMalloc (no counterpart in the reference).
  *

@@ -111,6 +111,17 @@ class Context:
     def use_graph(self, on: bool = True):
         abi.check(self._L.sph_use_graph(self._p, int(bool(on))))
 
+    def init_lattice(self, species_id: int, init, roles: int | None = None) -> int:
+        """Generates a species on the device from a setups.LatticeInit (lattice
+        blocks + profile) and sets it; returns its particle count."""
+        blocks, nb, prof = init.to_abi()
+        n = C.c_int64(0)
+        r = abi.SPECIES_ROLES[species_id] if roles is None else roles
+        abi.check(self._L.sph_init_lattice(self._p, int(species_id), int(r), int(nb), blocks, C.byref(prof),
+                                           C.byref(n)))
+        self._n[species_id] = int(n.value)
+        return int(n.value)
+
     def autotune(self, steps_per_trial: int = 2) -> dict:
         """Times every launch shape of the pair kernels on the current particles
         (the state is restored after each trial) and keeps the fastest."""
@@ -160,9 +171,14 @@ def run_one_step(ctx: Context, n_steps: int = 1, dt: float = 0.0):
     ctx.step(n_steps, dt)
 
 
-def context_for(workload) -> Context:
-    """A context holding every species of a :class:`spearhed_b200.setups.Workload`."""
+def context_for(workload, device_init: bool = False) -> Context:
+    """A context holding every species of a :class:`spearhed_b200.setups.Workload`;
+    with ``device_init`` the species are generated on the device from the
+    workload's lattice blocks (sph_init_lattice) instead of copied from the host."""
     ctx = Context(workload.params, workload.boxes)
     for sid, s in workload.species.items():
-        ctx.set_species(sid, s)
+        if device_init and sid in workload.init:
+            ctx.init_lattice(sid, workload.init[sid])
+        else:
+            ctx.set_species(sid, s)
     return ctx

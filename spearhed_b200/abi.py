@@ -183,6 +183,43 @@ class Species:
         return out
 
 
+MASK_NONE, MASK_INSIDE_DISC_XY, MASK_OUTSIDE_DISC_XY = 0, 1, 2
+PROFILE_CONSTANT, PROFILE_ORSZAG_TANG, PROFILE_KH_PERTURBATION, PROFILE_ROTOR = 0, 1, 2, 3
+
+
+class SphLatticeBlock(C.Structure):
+    _fields_ = [
+        ("lo", C.c_double * 3),
+        ("hi", C.c_double * 3),
+        ("counts", C.c_int32 * 3),
+        ("mask", C.c_int32),
+        ("spacing", C.c_double),
+        ("mask_centre", C.c_double * 2),
+        ("mask_radius", C.c_double),
+        ("box_id", C.c_int32),
+        ("jitter_group", C.c_int32),
+        ("jitter", C.c_double),
+        ("seed", C.c_uint64),
+        ("mass", C.c_double),
+        ("h", C.c_double),
+        ("density", C.c_double),
+        ("u", C.c_double),
+        ("psi", C.c_double),
+        ("vel", C.c_double * 3),
+        ("B", C.c_double * 3),
+    ]
+
+
+class SphInitProfile(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("wrap", C.c_int32 * 3),
+        ("wrap_lo", C.c_double * 3),
+        ("wrap_hi", C.c_double * 3),
+        ("p", C.c_double * 8),
+    ]
+
+
 class SphTuning(C.Structure):
     _fields_ = [
         ("density_variant", C.c_int32),
@@ -238,6 +275,10 @@ def lib():
         "sph_get_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_set_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_autotune": (C.c_int, [ctx_p, C.c_int32, P(SphTuning)]),
+        "sph_init_lattice": (C.c_int, [ctx_p, C.c_int32, C.c_uint32, C.c_int32, P(SphLatticeBlock),
+                                       P(SphInitProfile), P(C.c_int64)]),
+        "sph_sc_cell_counts": (C.c_int, [P(C.c_double), P(C.c_double), C.c_double, P(C.c_uint32)]),
+        "sph_sc_cell_counts_f32": (C.c_int, [P(C.c_float), P(C.c_float), C.c_float, P(C.c_uint32)]),
         "sph_set_tuning": (C.c_int, [ctx_p, C.c_int32, C.c_int32]),
         "sph_get_tuning": (C.c_int, [ctx_p, P(SphTuning)]),
         "sph_last_error_string": (C.c_char_p, []),

@@ -1088,6 +1088,30 @@ int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
 }
 
 // ============================================================== C ABI
+namespace
+{
+    //! Device buffers of one sph_init_lattice call, freed on every exit.
+    struct InitScratch
+    {
+        std::vector<void*> ptrs;
+        ~InitScratch()
+        {
+            for(void* p : ptrs)
+                cudaFree(p);
+        }
+        template<typename T>
+        cudaError_t take(T*& out, size_t count)
+        {
+            void* p = nullptr;
+            cudaError_t const e = cudaMalloc(&p, (count ? count : 1) * sizeof(T));
+            if(e == cudaSuccess)
+                ptrs.push_back(p);
+            out = static_cast<T*>(p);
+            return e;
+        }
+    };
+} // namespace
+
 extern "C" {
 
 int sph_default_params(SphParams* p)
@@ -1497,6 +1521,185 @@ int sph_use_graph(sph_ctx* ctx, int32_t on)
         return fail(SPH_ERR_INVALID, "null context");
     ctx->useGraph = on != 0;
     return SPH_OK;
+}
+
+
+int sph_init_lattice(
+    sph_ctx* ctx,
+    int32_t species_id,
+    uint32_t roles,
+    int32_t nblocks,
+    const SphLatticeBlock* blocks,
+    const SphInitProfile* profile,
+    int64_t* n_out)
+{
+    if(!ctx || species_id < 0 || species_id >= SPH_NUM_SPECIES || nblocks < 0 || (nblocks > 0 && !blocks))
+        return fail(SPH_ERR_INVALID, "sph_init_lattice: bad arguments");
+    SphInitProfile prof{};
+    if(profile)
+        prof = *profile;
+    if(prof.kind < SPH_PROFILE_CONSTANT || prof.kind > SPH_PROFILE_ROTOR)
+        return fail(SPH_ERR_INVALID, "sph_init_lattice: unknown profile");
+    // per-block lattice counts and site offsets; jitter groups of consecutive blocks
+    std::vector<sph::LatticeBlockDev> hb(static_cast<size_t>(nblocks));
+    std::vector<int> groupFirstBlock;
+    unsigned long long sites = 0;
+    for(int32_t b = 0; b < nblocks; ++b)
+    {
+        SphLatticeBlock const& B = blocks[b];
+        sph::LatticeBlockDev& d = hb[size_t(b)];
+        uint32_t n[3];
+        bool const given = B.counts[0] > 0 || B.counts[1] > 0 || B.counts[2] > 0;
+        for(int a = 0; a < 3; ++a)
+            if(!std::isfinite(B.lo[a]) || !std::isfinite(B.hi[a]) || !(B.hi[a] >= B.lo[a]))
+                return fail(SPH_ERR_INVALID, "sph_init_lattice: block with an invalid region");
+        if(given)
+        {
+            for(int a = 0; a < 3; ++a)
+            {
+                if(B.counts[a] <= 0)
+                    return fail(SPH_ERR_INVALID, "sph_init_lattice: counts must all be positive (or all 0)");
+                n[a] = uint32_t(B.counts[a]);
+            }
+        }
+        else
+        {
+            if(!(B.spacing > 0.0) || !std::isfinite(B.spacing))
+                return fail(SPH_ERR_INVALID, "sph_init_lattice: block needs counts or a positive spacing");
+            sph::latticeCounts(B.lo, B.hi, B.spacing, n);
+        }
+        if(B.mask < SPH_MASK_NONE || B.mask > SPH_MASK_OUTSIDE_DISC_XY)
+            return fail(SPH_ERR_INVALID, "sph_init_lattice: unknown mask");
+        if(B.box_id < 0)
+            return fail(SPH_ERR_INVALID, "sph_init_lattice: negative box id");
+        if(!(B.jitter >= 0.0) || !std::isfinite(B.jitter))
+            return fail(SPH_ERR_INVALID, "sph_init_lattice: jitter must be >= 0");
+        if(b == 0 || B.jitter_group != blocks[b - 1].jitter_group)
+            groupFirstBlock.push_back(b);
+        else if(B.jitter != blocks[b - 1].jitter || B.seed != blocks[b - 1].seed)
+            return fail(SPH_ERR_INVALID, "sph_init_lattice: blocks of one jitter group need one amplitude and seed");
+        for(int a = 0; a < 3; ++a)
+        {
+            d.lo[a] = B.lo[a];
+            d.n[a] = n[a];
+            d.d[a] = (B.hi[a] - B.lo[a]) / double(n[a]);
+            d.vel[a] = B.vel[a];
+            d.B[a] = B.B[a];
+        }
+        d.siteBase = sites;
+        d.mask = B.mask;
+        d.maskCentre[0] = B.mask_centre[0];
+        d.maskCentre[1] = B.mask_centre[1];
+        d.maskRadius = B.mask_radius;
+        d.box = B.box_id;
+        d.group = int32_t(groupFirstBlock.size() - 1);
+        d.mass = B.mass;
+        d.h = B.h;
+        d.density = B.density;
+        d.u = B.u;
+        d.psi = B.psi;
+        sites += (unsigned long long) n[0] * n[1] * n[2];
+    }
+    if(sites >= (1ull << 32))
+        return fail(SPH_ERR_UNSUPPORTED, "sph_init_lattice: more than 2^32 lattice sites");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    if(!ctx->stream)
+        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    cudaStream_t const s = ctx->stream;
+    uint32_t total = 0;
+    std::vector<uint32_t> first(size_t(nblocks) + 1, 0);
+    InitScratch scr;
+    sph::LatticeBlockDev* dBlocks = nullptr;
+    uint32_t *flags = nullptr, *ranks = nullptr, *scanScratch = nullptr, *dFirst = nullptr;
+    if(sites > 0)
+    {
+        SPH_CUDA_TRY(scr.take(dBlocks, hb.size()));
+        SPH_CUDA_TRY(scr.take(flags, sites));
+        SPH_CUDA_TRY(scr.take(ranks, sites));
+        SPH_CUDA_TRY(scr.take(scanScratch, sph::scanScratchWords(uint32_t(sites))));
+        SPH_CUDA_TRY(scr.take(dFirst, first.size()));
+        SPH_CUDA_TRY(cudaMemcpyAsync(dBlocks, hb.data(), sizeof(hb[0]) * hb.size(), cudaMemcpyHostToDevice, s));
+        sph::launchLatticeFlags(dBlocks, nblocks, sites, flags, s);
+        sph::exclusiveScan(flags, ranks, uint32_t(sites), scanScratch, s);
+        sph::launchBlockFirstRanks(dBlocks, nblocks, sites, flags, ranks, dFirst, s);
+        SPH_CUDA_TRY(cudaMemcpyAsync(first.data(), dFirst, 4 * first.size(), cudaMemcpyDeviceToHost, s));
+        SPH_CUDA_TRY(cudaStreamSynchronize(s));
+        total = first[size_t(nblocks)];
+    }
+    // jitter groups: particle range of each group
+    std::vector<sph::JitterGroupDev> groups(groupFirstBlock.size());
+    for(size_t g = 0; g < groups.size(); ++g)
+    {
+        int const b0 = groupFirstBlock[g];
+        int const b1 = g + 1 < groups.size() ? groupFirstBlock[g + 1] : nblocks;
+        groups[g].amplitude = blocks[b0].jitter;
+        groups[g].seed = blocks[b0].seed;
+        groups[g].first = first[size_t(b0)];
+        groups[g].count = first[size_t(b1)] - first[size_t(b0)];
+    }
+    // columns in species order, generated on the device
+    std::vector<std::vector<double>> host(kHostCols);
+    std::vector<int32_t> hostBox(total);
+    if(total > 0)
+    {
+        sph::InitColumns col{};
+        double* dcol[kHostCols];
+        for(int c = 0; c < kHostCols; ++c)
+            SPH_CUDA_TRY(scr.take(dcol[c], total));
+        for(int a = 0; a < 3; ++a)
+        {
+            col.x[a] = dcol[cX + a];
+            col.v[a] = dcol[cVX + a];
+            col.B[a] = dcol[cBX + a];
+        }
+        col.u = dcol[cU];
+        col.m = dcol[cM];
+        col.h = dcol[cH];
+        col.rho = dcol[cRho];
+        col.psi = dcol[cPsi];
+        SPH_CUDA_TRY(scr.take(col.box, total));
+        SPH_CUDA_TRY(scr.take(col.group, total));
+        sph::JitterGroupDev* dGroups = nullptr;
+        SPH_CUDA_TRY(scr.take(dGroups, groups.size()));
+        SPH_CUDA_TRY(
+            cudaMemcpyAsync(dGroups, groups.data(), sizeof(groups[0]) * groups.size(), cudaMemcpyHostToDevice, s));
+        sph::launchLatticePlace(dBlocks, nblocks, sites, flags, ranks, col, s);
+        sph::InitProfileDev pd{};
+        pd.kind = prof.kind;
+        for(int k = 0; k < 8; ++k)
+            pd.p[k] = prof.p[k];
+        for(int a = 0; a < 3; ++a)
+        {
+            pd.wrap[a] = prof.wrap[a];
+            pd.wrapLo[a] = prof.wrap_lo[a];
+            pd.wrapHi[a] = prof.wrap_hi[a];
+        }
+        sph::launchJitterProfile(col, total, dGroups, pd, s);
+        SPH_CUDA_TRY(cudaGetLastError());
+        for(int c = 0; c < kHostCols; ++c)
+        {
+            host[size_t(c)].resize(total);
+            SPH_CUDA_TRY(cudaMemcpyAsync(host[size_t(c)].data(), dcol[c], 8 * size_t(total), cudaMemcpyDeviceToHost, s));
+        }
+        SPH_CUDA_TRY(cudaMemcpyAsync(hostBox.data(), col.box, 4 * size_t(total), cudaMemcpyDeviceToHost, s));
+        SPH_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    SphSoAView v{};
+    for(int a = 0; a < 3; ++a)
+    {
+        v.pos[a] = host[size_t(cX + a)].data();
+        v.vel[a] = host[size_t(cVX + a)].data();
+        v.B[a] = host[size_t(cBX + a)].data();
+    }
+    v.mass = host[cM].data();
+    v.h = host[cH].data();
+    v.density = host[cRho].data();
+    v.u = host[cU].data();
+    v.psi = host[cPsi].data();
+    v.box_id = hostBox.data();
+    if(n_out)
+        *n_out = int64_t(total);
+    return sph_set_species(ctx, species_id, roles, int64_t(total), total > 0 ? &v : nullptr);
 }
 
 int sph_autotune(sph_ctx* ctx, int32_t steps_per_trial, SphTuning* out)

@@ -236,6 +236,76 @@ namespace sph
     void launchBoxReduce(DevCtx const& c, PhysArgs const& pa, double* out, double* scratch, cudaStream_t s);
     size_t boxReduceScratchDoubles(uint32_t nbox);
     void launchFill(double* p, size_t n, double v, cudaStream_t s);
+    // ---- init.cu: device initialiser of lattice blocks
+    //! One lattice block on the device (sites x-fastest, site s of the block at
+    //! lo + (i + 0.5) * d per axis).
+    struct LatticeBlockDev
+    {
+        double lo[3];
+        double d[3];
+        unsigned long long n[3];
+        unsigned long long siteBase; //!< first global site index of the block
+        int32_t mask;
+        double maskCentre[2];
+        double maskRadius;
+        int32_t box;
+        int32_t group; //!< jitter group
+        double mass, h, density, u, psi;
+        double vel[3], B[3];
+    };
+    struct JitterGroupDev
+    {
+        double amplitude;       //!< uniform displacement amplitude (length)
+        unsigned long long seed;
+        uint32_t first;         //!< first particle of the group
+        uint32_t count;         //!< particles in the group
+    };
+    struct InitProfileDev
+    {
+        int32_t kind;
+        double p[8];
+        int32_t wrap[3];
+        double wrapLo[3], wrapHi[3];
+    };
+    struct InitColumns
+    {
+        double* x[3];
+        double* v[3];
+        double* B[3];
+        double* m;
+        double* h;
+        double* rho;
+        double* u;
+        double* psi;
+        int32_t* box;
+        int32_t* group;
+    };
+    void latticeCounts(double const lo[3], double const hi[3], double spacing, uint32_t n[3]);
+    void launchLatticeFlags(LatticeBlockDev const* blocks, int nb, unsigned long long sites, uint32_t* flags, cudaStream_t s);
+    void launchLatticePlace(
+        LatticeBlockDev const* blocks,
+        int nb,
+        unsigned long long sites,
+        uint32_t const* flags,
+        uint32_t const* ranks,
+        InitColumns const& out,
+        cudaStream_t s);
+    //! first[b] = compacted index of block b's first kept site; first[nb] = total kept.
+    void launchBlockFirstRanks(
+        LatticeBlockDev const* blocks,
+        int nb,
+        unsigned long long sites,
+        uint32_t const* flags,
+        uint32_t const* ranks,
+        uint32_t* first,
+        cudaStream_t s);
+    void launchJitterProfile(
+        InitColumns const& out,
+        uint32_t n,
+        JitterGroupDev const* groups,
+        InitProfileDev const& prof,
+        cudaStream_t s);
+
     //! dst <- src for every master column (n particles).
     void launchCopyMaster(Master const& dst, Master const& src, uint32_t n, cudaStream_t s);
     //! master[p] = src[id[p]] for one species; badCount (or null) counts values

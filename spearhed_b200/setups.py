@@ -1,12 +1,19 @@
-"""Host-side initial conditions for the benchmark and test workloads.
+"""Initial conditions for the benchmark and test workloads, as lattice blocks.
 
 These play the part of the reference's setup blocks (SetupInterface +
 InitParticles + the SC lattice: include/spearhed/particles/initialization/
-InitParticles.hpp:284-433, spmacc/particles/initialization/SC.hpp:118-200,
-share/spearhed/ValidationSetups/SodShockTube.hpp:128-176): they place particles
-on simple-cubic lattices at cell centres, with equal masses, u = P/((gamma-1) rho).
-Jitter, where a workload asks for it, comes from numpy's Philox4x32-10
-counter-based generator keyed by the workload's seed.
+SetupInterface.hpp:34-113, InitParticles.hpp:284-433,
+spmacc/particles/initialization/SC.hpp:118-200,
+share/spearhed/ValidationSetups/SodShockTube.hpp:128-176).  Every workload is a
+list of :class:`LatticeBlock` (a region filled by a simple-cubic lattice at cell
+centres, with constant state and an optional keep-mask) plus a profile of
+analytic fields, a :class:`LatticeInit`.  The same description is generated two
+ways with the same arithmetic: on the host here (:meth:`LatticeInit.generate`,
+numpy) and on the device by ``sph_init_lattice`` (csrc/init.cu), which
+:func:`spearhed_b200.context_for` uses with ``device_init=True``.
+
+Jitter draws numpy's Philox4x64-10 (``Philox(key=seed).uniform(-1, 1)``) per
+jitter group: axis a of the group's particle i takes value a * n_group + i.
 
 Each generator returns a :class:`Workload`.
 """
@@ -21,6 +28,148 @@ from . import abi
 
 
 @dataclasses.dataclass
+class LatticeBlock:
+    """One region filled by an SC lattice (sites x-fastest, at lo + (i + 0.5) * ((hi - lo) / n))."""
+    lo: tuple
+    hi: tuple
+    counts: tuple = (0, 0, 0)   # sites per axis; all 0: from `spacing` (sc_counts)
+    spacing: float = 0.0
+    mask: int = abi.MASK_NONE
+    mask_centre: tuple = (0.0, 0.0)
+    mask_radius: float = 0.0
+    box_id: int = 0
+    group: int = 0              # consecutive blocks of a group share one jitter stream
+    jitter: float = 0.0         # uniform displacement amplitude (length) of the group
+    seed: int = 0
+    mass: float = 0.0
+    h: float = 0.0
+    density: float = 0.0
+    u: float = 0.0
+    psi: float = 0.0
+    vel: tuple = (0.0, 0.0, 0.0)
+    B: tuple = (0.0, 0.0, 0.0)
+
+    def lattice_counts(self):
+        if any(c > 0 for c in self.counts):
+            return tuple(int(c) for c in self.counts)
+        return sc_counts(self.lo, self.hi, self.spacing)
+
+
+@dataclasses.dataclass
+class LatticeInit:
+    """A species as lattice blocks plus a profile (abi.PROFILE_*, parameters, periodic wrap)."""
+    blocks: list
+    profile: int = abi.PROFILE_CONSTANT
+    params: tuple = ()
+    wrap: tuple = (0, 0, 0)
+    wrap_lo: tuple = (0.0, 0.0, 0.0)
+    wrap_hi: tuple = (0.0, 0.0, 0.0)
+
+    def to_abi(self):
+        arr = (abi.SphLatticeBlock * max(len(self.blocks), 1))()
+        for k, b in enumerate(self.blocks):
+            d = arr[k]
+            d.lo[:] = b.lo
+            d.hi[:] = b.hi
+            d.counts[:] = [int(c) for c in b.counts]
+            d.spacing = b.spacing
+            d.mask = b.mask
+            d.mask_centre[:] = b.mask_centre
+            d.mask_radius = b.mask_radius
+            d.box_id = b.box_id
+            d.jitter_group = b.group
+            d.jitter = b.jitter
+            d.seed = b.seed
+            d.mass, d.h, d.density, d.u, d.psi = b.mass, b.h, b.density, b.u, b.psi
+            d.vel[:] = b.vel
+            d.B[:] = b.B
+        prof = abi.SphInitProfile()
+        prof.kind = self.profile
+        prof.wrap[:] = list(self.wrap)
+        prof.wrap_lo[:] = list(self.wrap_lo)
+        prof.wrap_hi[:] = list(self.wrap_hi)
+        for k, v in enumerate(self.params):
+            prof.p[k] = v
+        return arr, len(self.blocks), prof
+
+    def generate(self) -> abi.Species:
+        """Host generation with the device initialiser's arithmetic and order."""
+        pos, state, groups = [], [], []
+        for b in self.blocks:
+            n = b.lattice_counts()
+            x = lattice(b.lo, b.hi, n)
+            if b.mask != abi.MASK_NONE:
+                r = np.hypot(x[0] - b.mask_centre[0], x[1] - b.mask_centre[1])
+                x = x[:, r < b.mask_radius] if b.mask == abi.MASK_INSIDE_DISC_XY else x[:, r >= b.mask_radius]
+            pos.append(x)
+            state.append((b, x.shape[1]))
+        x = np.concatenate(pos, axis=1) if pos else np.zeros((3, 0))
+        # jitter per group of consecutive blocks
+        off, k = 0, 0
+        while k < len(self.blocks):
+            g = self.blocks[k].group
+            kk, cnt = k, 0
+            while kk < len(self.blocks) and self.blocks[kk].group == g:
+                cnt += state[kk][1]
+                kk += 1
+            b0 = self.blocks[k]
+            if b0.jitter != 0.0 and cnt:
+                x[:, off:off + cnt] = x[:, off:off + cnt] + b0.jitter * philox_uniform(b0.seed, (3, cnt))
+            off += cnt
+            k = kk
+        for a in range(3):
+            if self.wrap[a]:
+                L = self.wrap_hi[a] - self.wrap_lo[a]
+                x[a] = self.wrap_lo[a] + (x[a] - self.wrap_lo[a]) % L
+        n = x.shape[1]
+        s = abi.Species(n)
+        s.pos[:] = x
+        off = 0
+        for b, cnt in state:
+            sl = slice(off, off + cnt)
+            s.mass[sl], s.h[sl], s.density[sl], s.u[sl], s.psi[sl] = b.mass, b.h, b.density, b.u, b.psi
+            for a in range(3):
+                s.vel[a, sl] = b.vel[a]
+                s.B[a, sl] = b.B[a]
+            s.box_id[sl] = b.box_id
+            off += cnt
+        p = self.params
+        if self.profile == abi.PROFILE_ORSZAG_TANG:
+            s.vel[0] = -np.sin(2 * math.pi * x[1])
+            s.vel[1] = np.sin(2 * math.pi * x[0])
+            s.B[0] = -p[0] * np.sin(2 * math.pi * x[1])
+            s.B[1] = p[0] * np.sin(4 * math.pi * x[0])
+        elif self.profile == abi.PROFILE_KH_PERTURBATION:
+            s.vel[1] = p[0] * np.sin(4 * math.pi * x[0])
+        elif self.profile == abi.PROFILE_ROTOR:
+            xc, yc, omega, r0, r1, width = p[:6]
+            r = np.hypot(x[0] - xc, x[1] - yc)
+            taper = np.clip((r1 - r) / width, 0.0, 1.0)
+            w = np.where(r < r0, omega, omega * taper)
+            s.vel[0] = -w * (x[1] - yc)
+            s.vel[1] = w * (x[0] - xc)
+        return s
+
+
+def _trunc_near_integer(v, eps):
+    """Truncation that snaps round-off just below an integer up (SC.hpp:49-58)."""
+    t = int(v)
+    tol = 4.0 * eps * (v if v > 1.0 else 1.0)
+    dist = float(t + 1) - v
+    return t + 1 if 0.0 <= dist <= tol else t
+
+
+def sc_counts(lo, hi, spacing):
+    """SC sites per axis (computeSCCellCounts, SC.hpp:98-132): axis 0 truncated
+    with a round-off snap, transverse axes rounded, each at least 1 (double)."""
+    n0 = _trunc_near_integer((hi[0] - lo[0]) / spacing, np.finfo(np.float64).eps)
+    out = [max(n0, 1)]
+    for a in (1, 2):
+        out.append(max(int((hi[a] - lo[a]) / spacing + 0.5), 1))
+    return tuple(out)
+
+
+@dataclasses.dataclass
 class Workload:
     name: str
     params: abi.SphParams
@@ -28,6 +177,7 @@ class Workload:
     species: dict  # species id -> abi.Species
     steps: int = 1
     meta: dict = dataclasses.field(default_factory=dict)
+    init: dict = dataclasses.field(default_factory=dict)  # species id -> LatticeInit (device initialiser input)
 
     @property
     def n(self):
@@ -56,9 +206,16 @@ class Workload:
         return out
 
 
+def _workload(name, params, boxes, inits, steps, meta):
+    """A workload whose species are generated on the host from their lattice blocks."""
+    return Workload(name, params, boxes, {sid: li.generate() for sid, li in inits.items()}, steps=steps,
+                    meta=meta, init=inits)
+
+
 def lattice(lo, hi, counts):
-    """Simple-cubic lattice at cell centres of the box lo..hi (SC.hpp:118-200)."""
-    axes = [lo[a] + (np.arange(counts[a]) + 0.5) * (hi[a] - lo[a]) / counts[a] for a in range(3)]
+    """Simple-cubic lattice at cell centres of the box lo..hi, x fastest
+    (SC.hpp:118-200: lo + (i + 0.5) * ((hi - lo) / n), each step rounded)."""
+    axes = [lo[a] + (np.arange(counts[a]) + 0.5) * ((hi[a] - lo[a]) / counts[a]) for a in range(3)]
     z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
     return np.stack([x.ravel(), y.ravel(), z.ravel()])
 
@@ -81,26 +238,19 @@ def sod_small(precision=abi.PREC_FP32_COMP, scale=1, reference_physics=False, hf
     nl = (int(64 * scale), int(16 * scale), int(16 * scale))
     nr = (int(32 * scale), int(8 * scale), int(8 * scale))
     Ly = 0.125
-    left = lattice((-0.5, 0.0, 0.0), (0.0, Ly, Ly), nl)
-    right = lattice((0.0, 0.0, 0.0), (0.5, Ly, Ly), nr)
     dxl, dxr = 0.5 / nl[0], 0.5 / nr[0]
     m = 1.0 * dxl ** 3
-    n = left.shape[1] + right.shape[1]
-    s = abi.Species(n)
-    s.pos[:] = np.concatenate([left, right], axis=1)
-    s.mass[:] = m
-    s.h[:] = np.concatenate([np.full(left.shape[1], hfact * dxl), np.full(right.shape[1], hfact * dxr)])
-    rho = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.125)])
-    P = np.concatenate([np.full(left.shape[1], 1.0), np.full(right.shape[1], 0.1)])
-    s.density[:] = rho
-    s.u[:] = P / ((gamma - 1.0) * rho)
+    left = LatticeBlock((-0.5, 0.0, 0.0), (0.0, Ly, Ly), counts=nl, mass=m, h=hfact * dxl, density=1.0,
+                        u=1.0 / ((gamma - 1.0) * 1.0))
+    right = LatticeBlock((0.0, 0.0, 0.0), (0.5, Ly, Ly), counts=nr, mass=m, h=hfact * dxr, density=0.125,
+                         u=0.1 / ((gamma - 1.0) * 0.125))
     physics = 0 if reference_physics else (abi.PHYS_AV | abi.PHYS_CFL | abi.PHYS_ADAPTIVE_H)
     params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
                                 physics=physics, gamma=gamma, h0=hfact * dxr, dt=1e-4, alpha=1.0, beta=2.0,
                                 cfl=0.3, hfact=hfact, h_max=1.5 * hfact * dxr)
     box = abi.make_box((-0.75, 0.0, 0.0), (0.75, Ly, Ly), (0, 1, 1))
-    return Workload("sod_small", params, [box], {abi.SPECIES_DEFAULT: s}, steps=50,
-                    meta={"n_left": left.shape[1], "n_right": right.shape[1], "dx_left": dxl, "dx_right": dxr})
+    return _workload("sod_small", params, [box], {abi.SPECIES_DEFAULT: LatticeInit([left, right])}, 50,
+                     {"n_left": int(np.prod(nl)), "n_right": int(np.prod(nr)), "dx_left": dxl, "dx_right": dxr})
 
 
 def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, jitter=0.0, seed=2):
@@ -117,34 +267,39 @@ def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, jitter=0
     gamma = 5.0 / 3.0
     dx = 1.0 / nx
     Lz = nz * dx
-    pos = lattice((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (nx, nx, nz))
-    if jitter > 0.0:
-        pos = pos + jitter * dx * philox_uniform(seed, pos.shape)
-        pos[0] %= 1.0
-        pos[1] %= 1.0
-        pos[2] %= Lz
-    n = pos.shape[1]
-    s = abi.Species(n)
-    s.pos[:] = pos
     rho0 = 25.0 / (36.0 * math.pi)
     P0 = 5.0 / (12.0 * math.pi)
-    s.mass[:] = rho0 * dx ** 3
-    s.h[:] = hfact * dx
-    s.density[:] = rho0
-    s.u[:] = P0 / ((gamma - 1.0) * rho0)
-    x, y = pos[0], pos[1]
-    s.vel[0] = -np.sin(2 * math.pi * y)
-    s.vel[1] = np.sin(2 * math.pi * x)
+    block = LatticeBlock((0.0, 0.0, 0.0), (1.0, 1.0, Lz), counts=(nx, nx, nz), jitter=jitter * dx if jitter > 0 else 0.0,
+                         seed=seed, mass=rho0 * dx ** 3, h=hfact * dx, density=rho0, u=P0 / ((gamma - 1.0) * rho0))
     b0 = 1.0 / math.sqrt(4 * math.pi)
-    s.B[0] = -b0 * np.sin(2 * math.pi * y)
-    s.B[1] = b0 * np.sin(4 * math.pi * x)
+    wrap = (1, 1, 1) if jitter > 0 else (0, 0, 0)
+    init = LatticeInit([block], abi.PROFILE_ORSZAG_TANG, (b0,), wrap=wrap, wrap_hi=(1.0, 1.0, Lz))
     physics = abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
     params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_GLOBAL,
                                 physics=physics, gamma=gamma, h0=hfact * dx, dt=2e-4, alpha=1.0, beta=2.0,
                                 cfl=0.3, dedner_sigma=1.0)
     box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (1, 1, 1))
-    return Workload("orszag_tang", params, [box], {abi.SPECIES_DEFAULT: s}, steps=200,
-                    meta={"nx": nx, "nz": nz, "dx": dx})
+    return _workload("orszag_tang", params, [box], {abi.SPECIES_DEFAULT: init}, 200, {"nx": nx, "nz": nz, "dx": dx})
+
+
+def _brio_wu_blocks(n_target, precision, nt, box_id):
+    gamma = 2.0
+    nxl = max(8, int(round(n_target / (nt * nt * 1.125))))
+    nxl += nxl % 2
+    dxl = 0.5 / nxl
+    L = nt * dxl
+    m = dxl ** 3
+    left = LatticeBlock((-0.5, 0.0, 0.0), (0.0, L, L), counts=(nxl, nt, nt), box_id=box_id, mass=m, h=1.2 * dxl,
+                        density=1.0, u=1.0 / ((gamma - 1.0) * 1.0), B=(0.75, 1.0, 0.0))
+    right = LatticeBlock((0.0, 0.0, 0.0), (0.5, L, L), counts=(nxl // 2, nt // 2, nt // 2), box_id=box_id, mass=m,
+                         h=2.4 * dxl, density=0.125, u=0.1 / ((gamma - 1.0) * 0.125), B=(0.75, -1.0, 0.0))
+    physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
+               | abi.PHYS_ADAPTIVE_H)
+    params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                physics=physics, gamma=gamma, h0=2.4 * dxl, dt=1e-5, alpha=1.0, beta=2.0,
+                                cfl=0.3, hfact=1.2, h_max=3.6 * dxl)
+    box = abi.make_box((-0.75, 0.0, 0.0), (0.75, L, L), (0, 1, 1))
+    return params, box, [left, right]
 
 
 def brio_wu_box(n_target=8192, precision=abi.PREC_FP32_COMP, nt=8, box_id=0):
@@ -157,58 +312,27 @@ def brio_wu_box(n_target=8192, precision=abi.PREC_FP32_COMP, nt=8, box_id=0):
     beyond each end).  Cubic spline, AV, SPMHD with Dedner cleaning and the
     tensile correction, adaptive h (hfact 1.2), CFL 0.3.
     """
-    gamma = 2.0
-    nxl = max(8, int(round(n_target / (nt * nt * 1.125))))
-    nxl += nxl % 2
-    dxl = 0.5 / nxl
-    L = nt * dxl
-    left = lattice((-0.5, 0.0, 0.0), (0.0, L, L), (nxl, nt, nt))
-    right = lattice((0.0, 0.0, 0.0), (0.5, L, L), (nxl // 2, nt // 2, nt // 2))
-    n = left.shape[1] + right.shape[1]
-    s = abi.Species(n)
-    s.pos[:] = np.concatenate([left, right], axis=1)
-    m = dxl ** 3
-    s.mass[:] = m
-    isl = np.concatenate([np.ones(left.shape[1], bool), np.zeros(right.shape[1], bool)])
-    rho = np.where(isl, 1.0, 0.125)
-    P = np.where(isl, 1.0, 0.1)
-    s.density[:] = rho
-    s.u[:] = P / ((gamma - 1.0) * rho)
-    s.h[:] = np.where(isl, 1.2 * dxl, 2.4 * dxl)
-    s.B[0] = 0.75
-    s.B[1] = np.where(isl, 1.0, -1.0)
-    s.box_id[:] = box_id
-    physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
-               | abi.PHYS_ADAPTIVE_H)
-    params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
-                                physics=physics, gamma=gamma, h0=2.4 * dxl, dt=1e-5, alpha=1.0, beta=2.0,
-                                cfl=0.3, hfact=1.2, h_max=3.6 * dxl)
-    box = abi.make_box((-0.75, 0.0, 0.0), (0.75, L, L), (0, 1, 1))
-    return params, box, s
+    params, box, blocks = _brio_wu_blocks(n_target, precision, nt, box_id)
+    return params, box, LatticeInit(blocks).generate()
 
 
 def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144):
     """An ensemble of independent Brio-Wu tubes with particle counts drawn
     log-uniform in [n_lo, n_hi] (numpy Philox, key ``seed``).  With the default
     512 boxes this is about 31 M particles.  Every box keeps its own time step.
-    The ensemble-wide h_max is the largest box's (it sets no cell size: each box
-    has its own grid from its own h)."""
+    The ensemble-wide h_max is 0, so each box sizes its grid from its own
+    largest h (x1.5 under adaptive h, within its periodic extent)."""
     rng = np.random.Generator(np.random.Philox(key=seed))
     sizes = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=nbox)).astype(int)
-    boxes, parts, params = [], [], None
-    hmax = 0.0
+    boxes, blocks, params = [], [], None
     for b, nb in enumerate(sizes):
-        p, box, s = brio_wu_box(int(nb), precision=precision, box_id=b)
+        p, box, bl = _brio_wu_blocks(int(nb), precision, 8, b)
         boxes.append(box)
-        parts.append(s)
-        hmax = max(hmax, p.h_max)
+        blocks.extend(bl)
         params = p
-    species = abi.Species.concat(parts)
-    # boxes differ in resolution; h_max = 0 lets each box size its grid from its own
-    # largest h (x1.5 under adaptive h)
     params.h_max = 0.0
-    return Workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: species}, steps=100,
-                    meta={"sizes": sizes.tolist(), "seed": seed})
+    return _workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: LatticeInit(blocks)}, 100,
+                     {"sizes": sizes.tolist(), "seed": seed})
 
 
 def kelvin_helmholtz(n_outer=224, n_band=282, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=3):
@@ -218,39 +342,32 @@ def kelvin_helmholtz(n_outer=224, n_band=282, precision=abi.PREC_FP32_COMP, hfac
     is a lattice whose spacing follows its density (n_band/n_outer ~ 2^(1/3);
     n_outer = 224, n_band = 282 give 5.62 M + 11.21 M = 16.8 M particles, masses
     within 0.5% of each other).  Uniform jitter of 0.05 spacing (Philox, key
-    ``seed``), vy = 0.01 sin(4 pi x), P = 2.5, gamma 5/3, Bx = 0.1.  Wendland C2,
-    h = hfact x local spacing (adaptive), AV, SPMHD with Dedner cleaning, CFL.
+    ``seed`` outside, ``seed`` + 1000 in the band), vy = 0.01 sin(4 pi x), P = 2.5,
+    gamma 5/3, Bx = 0.1.  Wendland C2, h = hfact x local spacing (adaptive), AV,
+    SPMHD with Dedner cleaning, CFL.
     """
     gamma = 5.0 / 3.0
     if n_outer % 4 or n_band % 2:
         raise ValueError("n_outer must be a multiple of 4 and n_band even (whole layers per slab)")
-    lo1 = lattice((0.0, 0.0, 0.0), (1.0, 0.25, 1.0), (n_outer, n_outer // 4, n_outer))
-    lo2 = lattice((0.0, 0.75, 0.0), (1.0, 1.0, 1.0), (n_outer, n_outer // 4, n_outer))
-    band = lattice((0.0, 0.25, 0.0), (1.0, 0.75, 1.0), (n_band, n_band // 2, n_band))
     d_o, d_b = 1.0 / n_outer, 1.0 / n_band
-    pos_o = np.concatenate([lo1, lo2], axis=1)
-    pos_o = pos_o + 0.05 * d_o * philox_uniform(seed, pos_o.shape)
-    pos_b = band + 0.05 * d_b * philox_uniform(seed + 1000, band.shape)
-    pos = np.concatenate([pos_o, pos_b], axis=1) % 1.0
-    n_o, n = pos_o.shape[1], pos_o.shape[1] + pos_b.shape[1]
-    s = abi.Species(n)
-    s.pos[:] = pos
-    isb = np.arange(n) >= n_o
-    s.mass[:] = np.where(isb, 2.0 * d_b ** 3, 1.0 * d_o ** 3)
-    s.density[:] = np.where(isb, 2.0, 1.0)
-    s.u[:] = 2.5 / ((gamma - 1.0) * s.density)
-    s.h[:] = hfact * np.where(isb, d_b, d_o)
-    s.vel[0] = np.where(isb, 0.5, -0.5)
-    s.vel[1] = 0.01 * np.sin(4 * math.pi * pos[0])
-    s.B[0] = 0.1
+    outer = dict(group=0, jitter=0.05 * d_o, seed=seed, mass=1.0 * d_o ** 3, h=hfact * d_o, density=1.0,
+                 u=2.5 / ((gamma - 1.0) * 1.0), vel=(-0.5, 0.0, 0.0), B=(0.1, 0.0, 0.0))
+    blocks = [
+        LatticeBlock((0.0, 0.0, 0.0), (1.0, 0.25, 1.0), counts=(n_outer, n_outer // 4, n_outer), **outer),
+        LatticeBlock((0.0, 0.75, 0.0), (1.0, 1.0, 1.0), counts=(n_outer, n_outer // 4, n_outer), **outer),
+        LatticeBlock((0.0, 0.25, 0.0), (1.0, 0.75, 1.0), counts=(n_band, n_band // 2, n_band), group=1,
+                     jitter=0.05 * d_b, seed=seed + 1000, mass=2.0 * d_b ** 3, h=hfact * d_b, density=2.0,
+                     u=2.5 / ((gamma - 1.0) * 2.0), vel=(0.5, 0.0, 0.0), B=(0.1, 0.0, 0.0)),
+    ]
+    init = LatticeInit(blocks, abi.PROFILE_KH_PERTURBATION, (0.01,), wrap=(1, 1, 1), wrap_hi=(1.0, 1.0, 1.0))
     physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
                | abi.PHYS_ADAPTIVE_H)
     params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_PAIR_MAX,
                                 physics=physics, gamma=gamma, h0=hfact * d_o, dt=1e-4, cfl=0.3, hfact=hfact,
                                 h_max=1.5 * hfact * d_o)
     box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (1, 1, 1))
-    return Workload("kelvin_helmholtz", params, [box], {abi.SPECIES_DEFAULT: s}, steps=100,
-                    meta={"n_outer": n_outer, "n_band": n_band})
+    return _workload("kelvin_helmholtz", params, [box], {abi.SPECIES_DEFAULT: init}, 100,
+                     {"n_outer": n_outer, "n_band": n_band})
 
 
 def mhd_rotor(nxy=1024, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=4):
@@ -268,40 +385,29 @@ def mhd_rotor(nxy=1024, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=4):
     gamma = 1.4
     Lz = nz / nxy
     dxa = 1.0 / nxy
-    amb = lattice((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (nxy, nxy, nz))
-    rr = np.hypot(amb[0] - 0.5, amb[1] - 0.5)
-    amb = amb[:, rr >= 0.1]
     nzd = int(round(nz * 10 ** (1.0 / 3.0)))
     nzd += 1 if nzd == nz * 2 else 0
     # in-plane lattice count per unit length giving ten times the ambient number density
     nd = int(round(np.sqrt(10.0 * nxy ** 3 * Lz / nzd)))
-    sq = lattice((0.4, 0.4, 0.0), (0.6, 0.6, Lz), (int(round(0.2 * nd)), int(round(0.2 * nd)), nzd))
-    disc = sq[:, np.hypot(sq[0] - 0.5, sq[1] - 0.5) < 0.1]
-    pos = np.concatenate([amb, disc], axis=1)
-    pos = pos + 0.05 * dxa * philox_uniform(seed, pos.shape)
-    pos[0] %= 1.0
-    pos[1] %= 1.0
-    pos[2] %= Lz
-    n = pos.shape[1]
-    s = abi.Species(n)
-    s.pos[:] = pos
     m = dxa ** 2 * (Lz / nz)  # ambient mass: rho 1 times the ambient cell volume
-    s.mass[:] = m
-    isd = np.arange(n) >= amb.shape[1]
-    s.density[:] = np.where(isd, 10.0, 1.0)
-    s.u[:] = 1.0 / ((gamma - 1.0) * s.density)
-    s.h[:] = hfact * np.cbrt(m / s.density)
-    r = np.hypot(pos[0] - 0.5, pos[1] - 0.5)
-    taper = np.clip((0.115 - r) / 0.015, 0.0, 1.0)
-    omega = np.where(r < 0.1, 20.0, 20.0 * taper)
-    s.vel[0] = -omega * (pos[1] - 0.5)
-    s.vel[1] = omega * (pos[0] - 0.5)
-    s.B[0] = 5.0 / math.sqrt(4 * math.pi)
+    Bx = 5.0 / math.sqrt(4 * math.pi)
+    common = dict(group=0, jitter=0.05 * dxa, seed=seed, mass=m, B=(Bx, 0.0, 0.0), mask_centre=(0.5, 0.5),
+                  mask_radius=0.1)
+    blocks = [
+        LatticeBlock((0.0, 0.0, 0.0), (1.0, 1.0, Lz), counts=(nxy, nxy, nz), mask=abi.MASK_OUTSIDE_DISC_XY,
+                     density=1.0, u=1.0 / ((gamma - 1.0) * 1.0), h=float(hfact * np.cbrt(m / 1.0)), **common),
+        LatticeBlock((0.4, 0.4, 0.0), (0.6, 0.6, Lz), counts=(int(round(0.2 * nd)), int(round(0.2 * nd)), nzd),
+                     mask=abi.MASK_INSIDE_DISC_XY, density=10.0, u=1.0 / ((gamma - 1.0) * 10.0),
+                     h=float(hfact * np.cbrt(m / 10.0)), **common),
+    ]
+    init = LatticeInit(blocks, abi.PROFILE_ROTOR, (0.5, 0.5, 20.0, 0.1, 0.115, 0.015), wrap=(1, 1, 1),
+                       wrap_hi=(1.0, 1.0, Lz))
     physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
                | abi.PHYS_ADAPTIVE_H)
     params = abi.default_params(kernel=abi.KERNEL_WENDLAND_C2, precision=precision, cull=abi.CULL_PAIR_MAX,
                                 physics=physics, gamma=gamma, h0=hfact * dxa, dt=1e-5, cfl=0.3, hfact=hfact,
                                 h_max=1.3 * hfact * dxa)
     box = abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, Lz), (1, 1, 1))
-    return Workload("mhd_rotor", params, [box], {abi.SPECIES_DEFAULT: s}, steps=150,
-                    meta={"nxy": nxy, "nz": nz, "n_disc": int(isd.sum())})
+    w = _workload("mhd_rotor", params, [box], {abi.SPECIES_DEFAULT: init}, 150, {"nxy": nxy, "nz": nz})
+    w.meta["n_disc"] = int(np.sum(w.species[abi.SPECIES_DEFAULT].density == 10.0))
+    return w
