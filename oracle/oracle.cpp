@@ -222,8 +222,9 @@ namespace orc
         }
     };
 
-    //! Cell edge >= rcell on every axis; n = floor(L / rcell) (at least 1).
-    inline int makeGrid(SphBox const& b, double rcell, Grid& g)
+    //! Cell edge >= rcell on every axis; n = floor(L / rcell), at least 1 and
+    //! at most nMax[a] when given.
+    inline int makeGrid(SphBox const& b, double rcell, Grid& g, int const* nMax = nullptr)
     {
         for(int a = 0; a < 3; ++a)
         {
@@ -234,6 +235,8 @@ namespace orc
                 return SPH_ERR_INVALID;
             double const nd = std::floor(g.L[a] / rcell);
             g.n[a] = nd < 1.0 ? 1 : (nd > 1.0e6 ? 1000000 : int(nd));
+            if(nMax && g.n[a] > nMax[a])
+                g.n[a] = nMax[a];
             g.edge[a] = g.L[a] / g.n[a];
             if(g.periodic[a] && g.L[a] < rcell)
                 return SPH_ERR_UNSUPPORTED; // images beyond the nearest would be needed
@@ -274,6 +277,7 @@ namespace orc
         std::vector<int64_t> cellStart; // CSR over global cells (sources only)
         std::vector<int64_t> cellItems;
         std::vector<double> hcap;
+        std::vector<int> nMax; // allocation of the first grid, per box and axis
         int64_t ncellTotal = 0;
 
         bool isTarget(int64_t i) const
@@ -307,41 +311,45 @@ namespace orc
             }
         }
         s.grids.resize(s.nbox);
-        s.hcap.assign(s.nbox, 0.0);
+        bool const first = s.nMax.empty();
+        bool const dynamic = s.p.cull == SPH_CULL_PAIR_MAX;
+        if(first)
+        {
+            s.nMax.assign(size_t(s.nbox) * 3, 1);
+            s.hcap.assign(s.nbox, 0.0);
+        }
         int64_t base = 0;
         for(int b = 0; b < s.nbox; ++b)
         {
-            // Same rule as the CUDA path: h_max when given, else the largest h
-            // (x1.5 under adaptive h); the oracle re-derives it every step, so
-            // adaptive-h parity runs pass h_max explicitly.
-            double hgrid = hmax[b];
-            if(s.p.cull == SPH_CULL_PAIR_MAX)
+            // Same rule as the CUDA path: the grid follows the box's current
+            // largest h (global cull: h0), its cell counts clamped to what the
+            // first grid allocates (room for h halving on every axis).  Adaptive
+            // h is capped by h_max, else by what the periodic axes admit.
+            if(dynamic && s.p.h_max > 0.0 && s.p.h_max < hmax[b])
+                return SPH_ERR_INVALID;
+            double const rc = cellRadius(sup, hmax[b]);
+            if(first)
             {
-                if(s.p.h_max > 0.0)
+                double hcap = s.p.h_max > 0.0 ? s.p.h_max : 1e300;
+                for(int a = 0; a < 3; ++a)
                 {
-                    if(s.p.h_max < hmax[b])
-                        return SPH_ERR_INVALID;
-                    hgrid = s.p.h_max;
+                    double const L = s.boxes[b].hi[a] - s.boxes[b].lo[a];
+                    double const nd = std::floor(L / rc);
+                    int const n0 = nd < 1.0 ? 1 : (nd > 1.0e6 ? 1000000 : int(nd));
+                    double const ndMax = dynamic ? std::floor(L / (0.5 * rc)) : nd;
+                    s.nMax[size_t(b) * 3 + a]
+                        = std::max(n0, ndMax < 1.0 ? 1 : (ndMax > 1.0e6 ? 1000000 : int(ndMax)));
+                    if(s.boxes[b].periodic[a] && s.p.h_max <= 0.0 && (s.p.physics & SPH_PHYS_ADAPTIVE_H))
+                    {
+                        double lim = L / (double(sup) * (1.0 + 1.0 / 262144.0));
+                        while(lim > hmax[b] && cellRadius(sup, lim) > L)
+                            lim = std::nextafter(lim, 0.0);
+                        hcap = std::min(hcap, std::max(lim, hmax[b]));
+                    }
                 }
-                else if(s.p.physics & SPH_PHYS_ADAPTIVE_H)
-                {
-                    // room to grow, clipped where a periodic axis would fall
-                    // below one cull radius (the kick caps h at hcap)
-                    double grow = 1.5 * hmax[b];
-                    for(int a = 0; a < 3; ++a)
-                        if(s.boxes[b].periodic[a])
-                        {
-                            double const L = s.boxes[b].hi[a] - s.boxes[b].lo[a];
-                            double lim = L / (double(sup) * (1.0 + 1.0 / 262144.0));
-                            while(lim > hmax[b] && cellRadius(sup, lim) > L)
-                                lim = std::nextafter(lim, 0.0);
-                            grow = std::min(grow, lim);
-                        }
-                    hgrid = std::max(hmax[b], grow);
-                }
+                s.hcap[b] = hcap;
             }
-            s.hcap[b] = hgrid;
-            int const st = makeGrid(s.boxes[b], cellRadius(sup, hgrid), s.grids[b]);
+            int const st = makeGrid(s.boxes[b], rc, s.grids[b], &s.nMax[size_t(b) * 3]);
             if(st != SPH_OK)
                 return st;
             s.grids[b].base = base;

@@ -162,7 +162,7 @@ struct sph_ctx
     bool mirrorStale = false;   //!< the host mirror is older than the device state
     bool densityValid = false;
     bool forceValid = false;
-    uint32_t n = 0, ncells = 0;
+    uint32_t n = 0, ncells = 0, activeCells = 0;
     uint32_t allocN = 0, allocCells = 0, allocBoxes = 0;
     std::vector<sph::BoxDev> boxDesc;
     sph::DevCtx dc{};
@@ -433,41 +433,22 @@ int sph_ctx::layout()
         }
     }
     boxDesc.assign(nbox, sph::BoxDev{});
-    uint64_t cellBase = 0;
+    uint64_t cellBase = 0, activeBase = 0;
+    bool const dynamic = p.cull == SPH_CULL_PAIR_MAX;
     for(int32_t b = 0; b < nbox; ++b)
     {
         SphBox const& B = boxes[b];
-        // The cell size admits h up to hgrid: h_max when given, else the largest
-        // input h (with 50% room to grow under adaptive h).
-        double hgrid = hmax[b];
-        if(p.cull == SPH_CULL_PAIR_MAX)
-        {
-            if(p.h_max > 0.0)
-            {
-                if(p.h_max < hmax[b])
-                    return fail(SPH_ERR_INVALID, "an input h exceeds params.h_max");
-                hgrid = p.h_max;
-            }
-            else if(p.physics & SPH_PHYS_ADAPTIVE_H)
-            {
-                // room to grow, but never past what a periodic axis admits (the
-                // kick caps h at hcap, so the grid stays valid)
-                double grow = 1.5 * hmax[b];
-                for(int a = 0; a < 3; ++a)
-                    if(B.periodic[a])
-                    {
-                        double const L = B.hi[a] - B.lo[a];
-                        double lim = L / (double(sup) * (1.0 + 1.0 / 262144.0));
-                        while(lim > hmax[b] && cellRadius(sup, lim) > L)
-                            lim = std::nextafter(lim, 0.0);
-                        grow = std::min(grow, lim);
-                    }
-                hgrid = std::max(hmax[b], grow);
-            }
-        }
+        // The grid follows the largest h of the box (global cull: h0).  With the
+        // pair-max cull it is re-derived every step from the current h, within an
+        // allocation that admits h shrinking by half on every axis.
+        double const hgrid = hmax[b];
+        if(dynamic && p.h_max > 0.0 && p.h_max < hmax[b])
+            return fail(SPH_ERR_INVALID, "an input h exceeds params.h_max");
         double const rc = cellRadius(sup, hgrid);
         sph::BoxDev& d = boxDesc[b];
-        uint64_t cells = 1;
+        uint64_t cells = 1, cellsMax = 1;
+        // adaptive h is capped by h_max, else by what the periodic axes admit
+        double hcap = p.h_max > 0.0 ? p.h_max : 1e300;
         for(int a = 0; a < 3; ++a)
         {
             d.lo[a] = B.lo[a];
@@ -477,19 +458,33 @@ int sph_ctx::layout()
             d.periodic[a] = B.periodic[a] ? 1 : 0;
             double const nd = std::floor(d.L[a] / rc);
             d.n[a] = nd < 1.0 ? 1 : (nd > 1.0e6 ? 1000000 : int32_t(nd));
+            double const ndMax = dynamic ? std::floor(d.L[a] / (0.5 * rc)) : nd;
+            d.nMax[a] = std::max(d.n[a], ndMax < 1.0 ? 1 : (ndMax > 1.0e6 ? 1000000 : int32_t(ndMax)));
             d.edge[a] = d.L[a] / d.n[a];
             d.edgef[a] = float(d.edge[a]);
             if(d.periodic[a] && d.L[a] < rc)
                 return fail(SPH_ERR_UNSUPPORTED, "periodic box thinner than the interaction radius");
+            if(d.periodic[a] && p.h_max <= 0.0 && (p.physics & SPH_PHYS_ADAPTIVE_H))
+            {
+                double lim = d.L[a] / (double(sup) * (1.0 + 1.0 / 262144.0));
+                while(lim > hmax[b] && cellRadius(sup, lim) > d.L[a])
+                    lim = std::nextafter(lim, 0.0);
+                hcap = std::min(hcap, std::max(lim, hmax[b]));
+            }
             cells *= uint64_t(d.n[a]);
+            cellsMax *= uint64_t(d.nMax[a]);
         }
         d.cellBase = uint32_t(cellBase);
         d.ncells = uint32_t(cells);
-        d.hcap = hgrid;
-        cellBase += cells;
+        d.ncellsMax = uint32_t(cellsMax);
+        d.activeBase = uint32_t(activeBase);
+        d.hcap = hcap;
+        cellBase += cellsMax;
+        activeBase += cells;
         if(cellBase * 2 + 1 >= (1ull << 32))
             return fail(SPH_ERR_UNSUPPORTED, "too many cells (2^31)");
     }
+    activeCells = uint32_t(activeBase);
     ncells = uint32_t(cellBase);
     return SPH_OK;
 }
@@ -533,7 +528,8 @@ int sph_ctx::allocate()
        || (st = alloc(dc.work, 1)))
         return st;
     if((st = alloc(dc.bs.dt, nbox)) || (st = alloc(dc.bs.time, nbox)) || (st = alloc(dc.bs.lastDt, nbox))
-       || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)))
+       || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)) || (st = alloc(dc.bs.hmaxBits, nbox))
+       || (st = alloc(dc.activeTotal, 1)))
         return st;
     dc.nPartialBlocks = sph::partialBlocks(n);
     if((st = alloc(dc.partials, size_t(dc.nPartialBlocks) * sph::kDiagWords))
@@ -596,6 +592,7 @@ int sph_ctx::uploadMirror()
             sh32[b * 32 + sl] = float4{float(o[0]) * d.edgef[0], float(o[1]) * d.edgef[1], float(o[2]) * d.edgef[2], 0.f};
             sh64[b * 32 + sl] = sph::D4{double(o[0]) * d.edge[0], double(o[1]) * d.edge[1], double(o[2]) * d.edge[2], 0.0};
         }
+    SPH_CUDA_TRY(cudaMemcpyAsync(dc.activeTotal, &activeCells, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
     SPH_CUDA_TRY(cudaMemcpyAsync(dc.shift32, sh32.data(), sizeof(float4) * sh32.size(), cudaMemcpyHostToDevice, stream));
     SPH_CUDA_TRY(cudaMemcpyAsync(dc.shift64, sh64.data(), sizeof(sph::D4) * sh64.size(), cudaMemcpyHostToDevice, stream));
     sph::StepScalars sc{};
@@ -713,6 +710,8 @@ int sph_ctx::build(bool drift)
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->candidates, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, sizeof(unsigned long long) * dc.nbox, stream));
+    if(p.cull == SPH_CULL_PAIR_MAX)
+        sph::launchGridUpdate(dc, supportOf(p.kernel), stream);
     sph::launchDriftKeys(dc, drift, stream);
     bool const inB = sph::radixSortPairs(dc.keysA, dc.valsA, dc.keysB, dc.valsB, n, dc.keyBits, dc.sortScratch, stream);
     uint32_t const* keys = inB ? dc.keysB : dc.keysA;

@@ -628,21 +628,24 @@ namespace sph
             double chMax = 0.0;
             int chBox = -1; // box whose c_h maximum chMax holds (warp-uniform)
 
-            // Work queue: each warp takes its next cell from a counter; the fetch
-            // for the next cell is issued first and read at the loop's end.
+            // Work queue over the cells of the boxes' current grids: each warp
+            // takes its next item from a counter; the fetch for the next item is
+            // issued first and read at the loop's end.  Item q is cell
+            // q - activeBase of the box whose range holds it.
+            uint32_t const nWork = *c.activeTotal;
             uint32_t pending = 0;
             if(lane == 0)
                 pending = atomicAdd(c.work, 1u);
-            for(uint32_t cell = __shfl_sync(0xffffffffu, pending, 0); cell < c.cells.ncells;
-                cell = __shfl_sync(0xffffffffu, pending, 0))
+            for(uint32_t q = __shfl_sync(0xffffffffu, pending, 0); q < nWork; q = __shfl_sync(0xffffffffu, pending, 0))
             {
                 if(lane == 0)
                     pending = atomicAdd(c.work, 1u);
+                int const box = boxOfWork(c.boxes, c.nbox, q);
+                uint32_t const cell = c.boxes[box].cellBase + (q - c.boxes[box].activeBase);
                 uint32_t const tBeg = c.cells.start[cell];
                 uint32_t const tEnd = c.cells.mid[cell];
                 if(tBeg >= tEnd)
                     continue;
-                int const box = boxOfCell(c.boxes, c.nbox, cell);
                 if(box != chBox)
                 {
                     // flush the previous box's signal-speed maximum

@@ -21,9 +21,12 @@ namespace sph
         float edgef[3];
         int32_t n[3];
         int32_t periodic[3];
-        uint32_t cellBase; //!< first global cell id of this box
-        uint32_t ncells;
-        double hcap; //!< largest h the cell size admits (adaptive h is capped here)
+        uint32_t cellBase; //!< first global cell id of this box (in the allocation)
+        uint32_t ncells;   //!< cells of the current grid (n[0] n[1] n[2])
+        double hcap;       //!< cap on adaptive h (params.h_max, else what the periodic axes admit)
+        int32_t nMax[3];   //!< allocated cells per axis: the current grid never exceeds them
+        uint32_t ncellsMax;
+        uint32_t activeBase; //!< first work item of this box (prefix of ncells over boxes)
     };
 
     //! Roles (include/spearhed_b200.h, SPH_ROLE_*).

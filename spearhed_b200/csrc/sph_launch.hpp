@@ -93,6 +93,21 @@ namespace sph
         fb[3] = mhd ? psi * inv2 : 0.0;
     }
 
+    //! Box of a density work item (boxes are sorted by activeBase).
+    __device__ __forceinline__ int boxOfWork(BoxDev const* boxes, uint32_t nbox, uint32_t q)
+    {
+        int lo = 0, hi = int(nbox) - 1;
+        while(lo < hi)
+        {
+            int const mid = (lo + hi + 1) >> 1;
+            if(boxes[mid].activeBase <= q)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+
     //! Box of a global cell id (boxes are sorted by cellBase).
     __device__ __forceinline__ int boxOfCell(BoxDev const* boxes, uint32_t nbox, uint32_t cell)
     {
@@ -170,6 +185,7 @@ namespace sph
         double* lastDt;              //!< dt of the last completed step
         unsigned long long* dtBits;  //!< min CFL dt over the box's targets (ordered bits)
         unsigned long long* chBits;  //!< max signal speed of the box's targets (ordered bits)
+        unsigned long long* hmaxBits; //!< max h of the box's particles (ordered bits; the grid follows it)
     };
 
     struct DevCtx
@@ -194,6 +210,7 @@ namespace sph
         uint32_t* sortScratch;
         uint32_t* status; //!< kStatWords words
         uint32_t* work;   //!< density work queue: next cell to hand out (zeroed before each launch)
+        uint32_t* activeTotal; //!< cells of the current grids of all boxes (the work items)
         StepScalars* scal;
         BoxScalars bs;
         double* partials; //!< per-block diagnostics partial sums
@@ -305,6 +322,11 @@ namespace sph
         JitterGroupDev const* groups,
         InitProfileDev const& prof,
         cudaStream_t s);
+
+    //! Grid of every box from its particles' current largest h (pair-max cull):
+    //! n = floor(L / cellRadius(support, hmax)) clamped to [1, nMax], the
+    //! stencil shift tables, the active-cell prefix and total.
+    void launchGridUpdate(DevCtx const& c, int support, cudaStream_t s);
 
     //! dst <- src for every master column (n particles).
     void launchCopyMaster(Master const& dst, Master const& src, uint32_t n, cudaStream_t s);

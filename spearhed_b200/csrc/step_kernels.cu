@@ -361,6 +361,88 @@ namespace sph
                 p[i] = v;
         }
 
+        //! Largest h of each box's particles, as ordered bits (one atomic per warp
+        //! when the warp is in one box).
+        __global__ void __launch_bounds__(kThreads) kBoxHmax(DevCtx c)
+        {
+            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
+            int const box = p < c.n ? c.cur.box[p] : -1;
+            double const h = p < c.n ? c.cur.h[p] : 0.0;
+            int const box0 = __shfl_sync(0xffffffffu, box, 0);
+            if(__all_sync(0xffffffffu, box == box0 || box < 0))
+            {
+                double m = h;
+#pragma unroll
+                for(int o = 16; o > 0; o >>= 1)
+                    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if((threadIdx.x & 31) == 0 && box0 >= 0)
+                    atomicMax(&c.bs.hmaxBits[box0], orderedBits(m));
+            }
+            else if(box >= 0)
+                atomicMax(&c.bs.hmaxBits[box], orderedBits(h));
+        }
+
+        //! Cell edge for cull radius support * h: the larger of the FP64 and FP32
+        //! radius widened by 2^-20 (the host's cellRadius, same rounding).
+        __device__ __forceinline__ double cellRadiusDev(int sup, double h)
+        {
+            double const r64 = __dmul_rn(double(sup), h);
+            double const r32 = double(__fmul_rn(float(sup), float(h)));
+            return __dmul_rn(r64 > r32 ? r64 : r32, 1.0 + 1.0 / 1048576.0);
+        }
+
+        //! Current grid of every box from its largest h (one block): cell counts
+        //! clamped to the allocation, edges, stencil shifts; then the prefix of
+        //! active cells over boxes (the density pass's work items).
+        __global__ void kGrid(DevCtx c, int sup)
+        {
+            for(uint32_t b = threadIdx.x; b < c.nbox; b += blockDim.x)
+            {
+                BoxDev& B = c.boxes[b];
+                double const h = __longlong_as_double(static_cast<long long>(c.bs.hmaxBits[b]));
+                if(h > 0.0)
+                {
+                    double const rc = cellRadiusDev(sup, h);
+                    uint32_t cells = 1;
+                    for(int a = 0; a < 3; ++a)
+                    {
+                        double const nd = floor(B.L[a] / rc);
+                        int n = nd < 1.0 ? 1 : (nd > double(B.nMax[a]) ? B.nMax[a] : int(nd));
+                        B.n[a] = n;
+                        B.edge[a] = B.L[a] / double(n);
+                        B.edgef[a] = float(B.edge[a]);
+                        cells *= uint32_t(n);
+                    }
+                    B.ncells = cells;
+                }
+                for(int sl = 0; sl < 32; ++sl)
+                {
+                    int const o[3] = {stencilOff(sl, 0), stencilOff(sl, 1), stencilOff(sl, 2)};
+                    bool const used = sl < 27;
+                    c.shift32[size_t(b) * 32 + sl] = used ? make_float4(
+                                                                float(o[0]) * B.edgef[0],
+                                                                float(o[1]) * B.edgef[1],
+                                                                float(o[2]) * B.edgef[2],
+                                                                0.f)
+                                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+                    c.shift64[size_t(b) * 32 + sl] = used ? D4{double(o[0]) * B.edge[0], double(o[1]) * B.edge[1],
+                                                                double(o[2]) * B.edge[2], 0.0}
+                                                          : D4{0.0, 0.0, 0.0, 0.0};
+                }
+            }
+            __syncthreads();
+            if(threadIdx.x == 0)
+            {
+                uint32_t base = 0;
+                for(uint32_t b = 0; b < c.nbox; ++b)
+                {
+                    c.boxes[b].activeBase = base;
+                    base += c.boxes[b].ncells;
+                }
+                *c.activeTotal = base;
+            }
+        }
+
         //! Copy of every master column (the state a step call starts from).
         __global__ void kCopyMaster(Master dst, Master src, uint32_t n)
         {
@@ -626,6 +708,18 @@ namespace sph
             kGatherSpeciesInt<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, master);
             countLaunches(1);
         }
+    }
+
+    void launchGridUpdate(DevCtx const& c, int support, cudaStream_t s)
+    {
+        cudaMemsetAsync(c.bs.hmaxBits, 0, sizeof(unsigned long long) * c.nbox, s);
+        if(c.n)
+        {
+            kBoxHmax<<<(c.n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+            countLaunches(1);
+        }
+        kGrid<<<1, 256, 0, s>>>(c, support);
+        countLaunches(1);
     }
 
     void launchCopyMaster(Master const& dst, Master const& src, uint32_t n, cudaStream_t s)
