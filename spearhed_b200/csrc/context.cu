@@ -406,6 +406,7 @@ int sph_ctx::layout()
     }
     int32_t const nbox = int32_t(boxes.size());
     std::vector<double> hmax(nbox, p.cull == SPH_CULL_PAIR_MAX ? 0.0 : p.h0);
+    std::vector<double> hmin(nbox, 1e300);
     for(auto& s : sp)
     {
         if(!s.set)
@@ -429,7 +430,10 @@ int sph_ctx::layout()
             if((s.roles & SPH_ROLE_SOURCE) && !(s.col[cM][i] > 0.0))
                 return fail(SPH_ERR_NONFINITE, "source particle mass must be positive");
             if(p.cull == SPH_CULL_PAIR_MAX)
+            {
                 hmax[b] = std::max(hmax[b], s.col[cH][i]);
+                hmin[b] = std::min(hmin[b], s.col[cH][i]);
+            }
         }
     }
     boxDesc.assign(nbox, sph::BoxDev{});
@@ -474,13 +478,20 @@ int sph_ctx::layout()
             cells *= uint64_t(d.n[a]);
             cellsMax *= uint64_t(d.nMax[a]);
         }
+        // Boxes whose h spans a factor of two or more also allocate level-1 cells
+        // (2x2x2 per level-0 cell) for the particles whose cull radius fits half
+        // a cell; the grid update decides each step whether they are used.
+        d.levelsAlloc = dynamic && hmin[b] <= 0.5 * hmax[b] ? 2 : 1;
+        d.e1 = 0.5 * std::min(d.edge[0], std::min(d.edge[1], d.edge[2]));
+        d.levels = d.levelsAlloc == 2 && cellRadius(sup, hmin[b]) <= d.e1 ? 2 : 1;
         d.cellBase = uint32_t(cellBase);
         d.ncells = uint32_t(cells);
         d.ncellsMax = uint32_t(cellsMax);
+        d.nItems = uint32_t(d.levels == 2 ? 9 * cells : cells);
         d.activeBase = uint32_t(activeBase);
         d.hcap = hcap;
-        cellBase += cellsMax;
-        activeBase += cells;
+        cellBase += d.levelsAlloc == 2 ? 9 * cellsMax : cellsMax;
+        activeBase += d.nItems;
         if(cellBase * 2 + 1 >= (1ull << 32))
             return fail(SPH_ERR_UNSUPPORTED, "too many cells (2^31)");
     }
@@ -496,6 +507,7 @@ int sph_ctx::allocate()
     uint32_t const nbox = uint32_t(boxDesc.size());
     dc.n = n;
     dc.nbox = nbox;
+    dc.support = supportOf(p.kernel);
     int st = SPH_OK;
     if((st = alloc(dc.boxes, nbox)) || (st = alloc(dc.shift32, size_t(nbox) * 32))
        || (st = alloc(dc.shift64, size_t(nbox) * 32)) || (st = allocMaster(dc.cur)) || (st = allocMaster(dc.alt)))
@@ -529,7 +541,7 @@ int sph_ctx::allocate()
         return st;
     if((st = alloc(dc.bs.dt, nbox)) || (st = alloc(dc.bs.time, nbox)) || (st = alloc(dc.bs.lastDt, nbox))
        || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)) || (st = alloc(dc.bs.hmaxBits, nbox))
-       || (st = alloc(dc.activeTotal, 1)))
+       || (st = alloc(dc.bs.hminBits, nbox)) || (st = alloc(dc.activeTotal, 1)))
         return st;
     dc.nPartialBlocks = sph::partialBlocks(n);
     if((st = alloc(dc.partials, size_t(dc.nPartialBlocks) * sph::kDiagWords))

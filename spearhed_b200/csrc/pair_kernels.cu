@@ -641,7 +641,10 @@ namespace sph
                 if(lane == 0)
                     pending = atomicAdd(c.work, 1u);
                 int const box = boxOfWork(c.boxes, c.nbox, q);
-                uint32_t const cell = c.boxes[box].cellBase + (q - c.boxes[box].activeBase);
+                // item -> cell: the box's level-0 cells first, then its level-1 cells
+                uint32_t const l = q - c.boxes[box].activeBase;
+                uint32_t const nc0 = c.boxes[box].ncells;
+                uint32_t const cell = c.boxes[box].cellBase + (l < nc0 ? l : c.boxes[box].ncellsMax + (l - nc0));
                 uint32_t const tBeg = c.cells.start[cell];
                 uint32_t const tEnd = c.cells.mid[cell];
                 if(tBeg >= tEnd)
@@ -656,50 +659,78 @@ namespace sph
                     chBox = box;
                 }
                 BoxDev const& B = c.boxes[box];
-                uint32_t const lc = cell - B.cellBase;
-                int const cc[3]
-                    = {int(lc % uint32_t(B.n[0])), int((lc / uint32_t(B.n[0])) % uint32_t(B.n[1])),
-                       int(lc / (uint32_t(B.n[0]) * uint32_t(B.n[1])))};
-                // Lane l < 27 describes stencil slot l: its source range and image shift.
-                uint32_t sBeg = 0, sCnt = 0;
-                T sh[3] = {T(0), T(0), T(0)};
-                if(lane < 27)
+                // Target cell: level 0 (the grid) or level 1 (the 2x2x2 sub-cells of
+                // a level-0 cell), its coordinates in its level and its level-0 parent.
+                int const lt = l < B.ncells ? 0 : 1;
+                int ct[3], c0[3];
                 {
+                    uint32_t const li = lt ? l - B.ncells : l;
+                    uint32_t const n0 = uint32_t(B.n[0]) << lt, n1 = uint32_t(B.n[1]) << lt;
+                    ct[0] = int(li % n0);
+                    ct[1] = int((li / n0) % n1);
+                    ct[2] = int(li / (n0 * n1));
+#pragma unroll
+                    for(int a = 0; a < 3; ++a)
+                        c0[a] = ct[a] >> lt;
+                }
+                // Candidate descriptors: the 27 level-0 cells around the parent, then
+                // with two levels the 27 level-1 cells around a level-1 target or the
+                // 216 level-1 sub-cells of those 27 cells for a level-0 target.  Each
+                // carries its source range and the level-0 stencil slot of its image.
+                int const nDesc = 27 + (B.levels == 2 ? (lt ? 27 : 216) : 0);
+                int const selfDesc = lt ? 27 + kCentreSlot : kCentreSlot;
+                auto describe = [&](int d, uint32_t& sBeg, uint32_t& sCnt, uint32_t& slot, T sh[3])
+                {
+                    sBeg = 0;
+                    sCnt = 0;
+                    slot = 0;
+                    sh[0] = sh[1] = sh[2] = T(0);
+                    if(d >= nDesc)
+                        return;
+                    int o[3], f[3];
                     bool ok = true;
-                    int nc[3];
+                    bool const fine = d >= 27;
+                    int const k = d - 27;
+                    int const on = d < 27 ? d : (lt ? 0 : (k >> 3)); // level-0 neighbour of the coarse paths
 #pragma unroll
                     for(int a = 0; a < 3; ++a)
                     {
-                        int const o = stencilOff(lane, a);
-                        nc[a] = cc[a] + o;
-                        if(nc[a] < 0 || nc[a] >= B.n[a])
+                        int const n0 = B.n[a];
+                        if(fine && lt)
                         {
-                            if(B.periodic[a])
-                                nc[a] = (nc[a] + B.n[a]) % B.n[a];
-                            else
-                                ok = false;
+                            // level-1 neighbour of a level-1 target
+                            int const fa = ct[a] + stencilOff(k, a);
+                            o[a] = (fa >> 1) - c0[a];
+                            int const n1 = 2 * n0;
+                            f[a] = fa < 0 || fa >= n1 ? (B.periodic[a] ? (fa + n1) % n1 : -1) : fa;
+                            ok = ok && f[a] >= 0;
                         }
-                        sh[a] = T(o) * edgeOf<T>(B, a);
+                        else
+                        {
+                            o[a] = stencilOff(on, a);
+                            int ca = c0[a] + o[a];
+                            if(ca < 0 || ca >= n0)
+                            {
+                                if(B.periodic[a])
+                                    ca = (ca + n0) % n0;
+                                else
+                                    ok = false;
+                            }
+                            f[a] = fine ? 2 * ca + ((k >> a) & 1) : ca; // sub-cell k & 7 of a level-0 neighbour
+                        }
                     }
-                    if(ok)
-                    {
-                        uint32_t const ncell
-                            = B.cellBase + (uint32_t(nc[2]) * uint32_t(B.n[1]) + uint32_t(nc[1])) * uint32_t(B.n[0])
-                              + uint32_t(nc[0]);
-                        sBeg = c.cells.start[ncell];
-                        sCnt = c.cells.end[ncell] - sBeg;
-                    }
-                }
-                uint32_t incl = sCnt;
+                    slot = uint32_t((o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1));
 #pragma unroll
-                for(int d = 1; d < 32; d <<= 1)
-                {
-                    uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
-                    if(lane >= d)
-                        incl += o;
-                }
-                uint32_t const pre = incl - sCnt;
-                uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+                    for(int a = 0; a < 3; ++a)
+                        sh[a] = T(o[a]) * edgeOf<T>(B, a);
+                    if(!ok)
+                        return;
+                    uint32_t const m0 = uint32_t(B.n[0]) << (fine ? 1 : 0), m1 = uint32_t(B.n[1]) << (fine ? 1 : 0);
+                    uint32_t const idx = (uint32_t(f[2]) * m1 + uint32_t(f[1])) * m0 + uint32_t(f[0]);
+                    uint32_t const cellId = B.cellBase + (fine ? B.ncellsMax : 0u) + idx;
+                    sBeg = c.cells.start[cellId];
+                    sCnt = c.cells.end[cellId] - sBeg;
+                };
 
                 // Two target chunks (up to 64 targets) share every staged window.
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
@@ -708,17 +739,35 @@ namespace sph
                     initChunk(A, rec, tc, tEnd, lane);
                     bool const twoChunks = tc + 32 < tEnd;
                     initChunk(Bc, rec, tc + 32, tEnd, lane);
+                    for(int page = 0; page * 32 < nDesc; ++page)
+                    {
+                    uint32_t sBeg, sCnt, slotD;
+                    T sh[3];
+                    describe(page * 32 + lane, sBeg, sCnt, slotD, sh);
+                    int const nsl = min(32, nDesc - page * 32);
+                    uint32_t incl = sCnt;
+#pragma unroll
+                    for(int d = 1; d < 32; d <<= 1)
+                    {
+                        uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
+                        if(lane >= d)
+                            incl += o;
+                    }
+                    uint32_t const pre = incl - sCnt;
+                    uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+                    int const selfLane = selfDesc - page * 32;
                     for(uint32_t cb = 0; cb < total; cb += CAP)
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
                         __syncwarp();
-                        for(int sl = 0; sl < 27; ++sl)
+                        for(int sl = 0; sl < nsl; ++sl)
                         {
                             uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
                             uint32_t const n0 = __shfl_sync(0xffffffffu, sCnt, sl);
                             if(p0 + n0 <= cb || p0 >= ce)
-                                continue; // uniform: slot outside this window
+                                continue; // uniform: descriptor outside this window
                             uint32_t const b0 = __shfl_sync(0xffffffffu, sBeg, sl);
+                            uint32_t const slotS = __shfl_sync(0xffffffffu, slotD, sl);
                             T const sx = __shfl_sync(0xffffffffu, sh[0], sl);
                             T const sy = __shfl_sync(0xffffffffu, sh[1], sl);
                             T const sz = __shfl_sync(0xffffffffu, sh[2], sl);
@@ -731,7 +780,7 @@ namespace sph
                                 sNX[q - cb] = -addRn(pj.x, sx);
                                 sNY[q - cb] = -addRn(pj.y, sy);
                                 sNZ[q - cb] = -addRn(pj.z, sz);
-                                sEnt[q - cb] = packEntry(j, uint32_t(sl));
+                                sEnt[q - cb] = packEntry(j, slotS);
                                 if constexpr(PAIRMAX)
                                     sH[q - cb] = rec.hc[j];
                             }
@@ -747,13 +796,15 @@ namespace sph
                                 sH[q] = T(0);
                         }
                         __syncwarp();
-                        // staged index of a target = centre slot's window offset + its rank in the cell
-                        uint32_t const cPre = __shfl_sync(0xffffffffu, pre, kCentreSlot);
-                        uint32_t const cBeg = __shfl_sync(0xffffffffu, sBeg, kCentreSlot);
+                        // staged index of a target = its own cell's window offset + its rank
+                        // in the cell, on the page that holds its own cell
+                        bool const selfPage = selfLane >= 0 && selfLane < 32;
+                        uint32_t const cPre = __shfl_sync(0xffffffffu, pre, selfPage ? selfLane : 0);
+                        uint32_t const cBeg = __shfl_sync(0xffffffffu, sBeg, selfPage ? selfLane : 0);
                         auto selfIndex = [&](uint32_t t) -> uint32_t
                         {
                             uint32_t const q = cPre + (t - cBeg);
-                            return (q >= cb && q < ce) ? q - cb : 0xffffffffu;
+                            return (selfPage && q >= cb && q < ce) ? q - cb : 0xffffffffu;
                         };
                         cullChunk<V4, T, PAIRMAX>(
                             A, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(A.t), supT, R2g, c.lists.list, cap, countOnly);
@@ -763,6 +814,7 @@ namespace sph
                                 countOnly);
                     }
                     cand += uint64_t(total) * (min(32u, tEnd - tc) + (twoChunks ? min(32u, tEnd - tc - 32) : 0u));
+                    }
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
                     pairs += (leadA ? A.nl : 0u) + (leadB ? Bc.nl : 0u);

@@ -25,8 +25,12 @@ namespace sph
         uint32_t ncells;   //!< cells of the current grid (n[0] n[1] n[2])
         double hcap;       //!< cap on adaptive h (params.h_max, else what the periodic axes admit)
         int32_t nMax[3];   //!< allocated cells per axis: the current grid never exceeds them
-        uint32_t ncellsMax;
-        uint32_t activeBase; //!< first work item of this box (prefix of ncells over boxes)
+        uint32_t ncellsMax; //!< allocated level-0 cells; level-1 cells (8 per level-0 cell) follow them
+        uint32_t activeBase; //!< first work item of this box (prefix of items over boxes)
+        uint32_t nItems;     //!< work items: ncells, times 9 with two levels
+        int32_t levelsAlloc; //!< 2 when level-1 cells are allocated
+        int32_t levels;      //!< 2 when this step bins small-h particles into level-1 cells
+        double e1;           //!< level-1 cell edge bound: a particle whose cell radius fits it is level 1
     };
 
     //! Roles (include/spearhed_b200.h, SPH_ROLE_*).
@@ -40,6 +44,15 @@ namespace sph
     }
 
     //! Cell coordinate along one axis: floor((x - lo)/edge) clamped to [0, n-1].
+    //! Cell edge for cull radius support * h: the larger of the FP64 and FP32
+    //! radius widened by 2^-20 (the host's cellRadius, same rounding).
+    __device__ __forceinline__ double cellRadiusDev(int sup, double h)
+    {
+        double const r64 = __dmul_rn(double(sup), h);
+        double const r32 = double(__fmul_rn(float(sup), float(h)));
+        return __dmul_rn(r64 > r32 ? r64 : r32, 1.0 + 1.0 / 1048576.0);
+    }
+
     __device__ __forceinline__ int cellCoord(BoxDev const& b, int a, double x)
     {
         double const f = floor((x - b.lo[a]) / b.edge[a]);

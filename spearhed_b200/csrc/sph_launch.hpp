@@ -186,6 +186,7 @@ namespace sph
         unsigned long long* dtBits;  //!< min CFL dt over the box's targets (ordered bits)
         unsigned long long* chBits;  //!< max signal speed of the box's targets (ordered bits)
         unsigned long long* hmaxBits; //!< max h of the box's particles (ordered bits; the grid follows it)
+        unsigned long long* hminBits; //!< min h of the box's particles (ordered bits; two levels when small enough)
     };
 
     struct DevCtx
@@ -210,7 +211,8 @@ namespace sph
         uint32_t* sortScratch;
         uint32_t* status; //!< kStatWords words
         uint32_t* work;   //!< density work queue: next cell to hand out (zeroed before each launch)
-        uint32_t* activeTotal; //!< cells of the current grids of all boxes (the work items)
+        uint32_t* activeTotal; //!< work items of all boxes (their current cells, both levels)
+        int32_t support;       //!< kernel support in units of h
         StepScalars* scal;
         BoxScalars bs;
         double* partials; //!< per-block diagnostics partial sums

@@ -66,11 +66,26 @@ namespace sph
                     atomicAdd(&c.status[kStatOutside], 1u);
                 if(isSource(role))
                 {
-                    int const cx = cellCoord(B, 0, x[0]);
-                    int const cy = cellCoord(B, 1, x[1]);
-                    int const cz = cellCoord(B, 2, x[2]);
-                    uint32_t const cell = B.cellBase + (uint32_t(cz) * uint32_t(B.n[1]) + uint32_t(cy)) * uint32_t(B.n[0])
-                                          + uint32_t(cx);
+                    int cc[3];
+#pragma unroll
+                    for(int a = 0; a < 3; ++a)
+                        cc[a] = cellCoord(B, a, x[a]);
+                    uint32_t cell = B.cellBase + (uint32_t(cc[2]) * uint32_t(B.n[1]) + uint32_t(cc[1])) * uint32_t(B.n[0])
+                                    + uint32_t(cc[0]);
+                    if(B.levels == 2 && cellRadiusDev(c.support, c.cur.h[p]) <= B.e1)
+                    {
+                        // level 1: the 2x2x2 sub-cell of the level-0 cell, from the
+                        // position relative to the cell corner (as the permute computes it)
+                        int f[3];
+#pragma unroll
+                        for(int a = 0; a < 3; ++a)
+                        {
+                            double const rel = x[a] - (B.lo[a] + double(cc[a]) * B.edge[a]);
+                            f[a] = 2 * cc[a] + (rel >= 0.5 * B.edge[a] ? 1 : 0);
+                        }
+                        uint32_t const m0 = 2u * uint32_t(B.n[0]), m1 = 2u * uint32_t(B.n[1]);
+                        cell = B.cellBase + B.ncellsMax + (uint32_t(f[2]) * m1 + uint32_t(f[1])) * m0 + uint32_t(f[0]);
+                    }
                     key = 2u * cell + (isTarget(role) ? 0u : 1u);
                 }
             }
@@ -371,24 +386,24 @@ namespace sph
             int const box0 = __shfl_sync(0xffffffffu, box, 0);
             if(__all_sync(0xffffffffu, box == box0 || box < 0))
             {
-                double m = h;
+                double m = box >= 0 ? h : 0.0, mn = box >= 0 ? h : 1e300;
 #pragma unroll
                 for(int o = 16; o > 0; o >>= 1)
+                {
                     m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                }
                 if((threadIdx.x & 31) == 0 && box0 >= 0)
+                {
                     atomicMax(&c.bs.hmaxBits[box0], orderedBits(m));
+                    atomicMin(&c.bs.hminBits[box0], orderedBits(mn));
+                }
             }
             else if(box >= 0)
+            {
                 atomicMax(&c.bs.hmaxBits[box], orderedBits(h));
-        }
-
-        //! Cell edge for cull radius support * h: the larger of the FP64 and FP32
-        //! radius widened by 2^-20 (the host's cellRadius, same rounding).
-        __device__ __forceinline__ double cellRadiusDev(int sup, double h)
-        {
-            double const r64 = __dmul_rn(double(sup), h);
-            double const r32 = double(__fmul_rn(float(sup), float(h)));
-            return __dmul_rn(r64 > r32 ? r64 : r32, 1.0 + 1.0 / 1048576.0);
+                atomicMin(&c.bs.hminBits[box], orderedBits(h));
+            }
         }
 
         //! Current grid of every box from its largest h (one block): cell counts
@@ -415,6 +430,14 @@ namespace sph
                     }
                     B.ncells = cells;
                 }
+                // two levels when the box allocates them and its smallest h fits half a cell
+                double e1 = 0.5 * B.edge[0];
+                e1 = fmin(e1, 0.5 * B.edge[1]);
+                e1 = fmin(e1, 0.5 * B.edge[2]);
+                B.e1 = e1;
+                double const hmin = __longlong_as_double(static_cast<long long>(c.bs.hminBits[b]));
+                B.levels = (B.levelsAlloc == 2 && hmin > 0.0 && hmin < 1e300 && cellRadiusDev(sup, hmin) <= e1) ? 2 : 1;
+                B.nItems = B.levels == 2 ? 9u * B.ncells : B.ncells;
                 for(int sl = 0; sl < 32; ++sl)
                 {
                     int const o[3] = {stencilOff(sl, 0), stencilOff(sl, 1), stencilOff(sl, 2)};
@@ -437,7 +460,7 @@ namespace sph
                 for(uint32_t b = 0; b < c.nbox; ++b)
                 {
                     c.boxes[b].activeBase = base;
-                    base += c.boxes[b].ncells;
+                    base += c.boxes[b].nItems;
                 }
                 *c.activeTotal = base;
             }
@@ -473,9 +496,9 @@ namespace sph
             __shared__ uint32_t lo[kThreads], hi[kThreads];
             BoxDev const& B = c.boxes[blockIdx.x];
             uint32_t l = 0xffffffffu, h = 0;
-            for(uint32_t lc = threadIdx.x; lc < B.ncells; lc += kThreads)
+            for(uint32_t lc = threadIdx.x; lc < B.nItems; lc += kThreads)
             {
-                uint32_t const cell = B.cellBase + lc;
+                uint32_t const cell = B.cellBase + (lc < B.ncells ? lc : B.ncellsMax + (lc - B.ncells));
                 uint32_t const s = c.cells.start[cell], e = c.cells.end[cell];
                 if(e > s)
                 {
@@ -713,6 +736,7 @@ namespace sph
     void launchGridUpdate(DevCtx const& c, int support, cudaStream_t s)
     {
         cudaMemsetAsync(c.bs.hmaxBits, 0, sizeof(unsigned long long) * c.nbox, s);
+        cudaMemsetAsync(c.bs.hminBits, 0xff, sizeof(unsigned long long) * c.nbox, s);
         if(c.n)
         {
             kBoxHmax<<<(c.n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
