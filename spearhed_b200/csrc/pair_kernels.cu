@@ -41,12 +41,14 @@ namespace sph
         {
             using V4 = float4;
             static constexpr int cap = 256;
+            static constexpr int kStageBatch = 2; //!< staged positions per lane with loads in flight
         };
         template<>
         struct PairCfg<double>
         {
             using V4 = D4;
             static constexpr int cap = 256;
+            static constexpr int kStageBatch = 2;
         };
 
         template<typename T>
@@ -732,6 +734,27 @@ namespace sph
                     sCnt = c.cells.end[cellId] - sBeg;
                 };
 
+                // exclusive prefix of the page's source counts and the page total
+                auto scan = [&](uint32_t cnt, uint32_t& pre, uint32_t& total)
+                {
+                    uint32_t incl = cnt;
+#pragma unroll
+                    for(int d = 1; d < 32; d <<= 1)
+                    {
+                        uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
+                        if(lane >= d)
+                            incl += o;
+                    }
+                    pre = incl - cnt;
+                    total = __shfl_sync(0xffffffffu, incl, 31);
+                };
+                // Page 0 (all of a single-level box's 27 slots) is described once per
+                // cell; later pages once per target chunk.
+                uint32_t sBeg0, sCnt0, slot0, pre0, total0;
+                T sh0[3];
+                describe(lane, sBeg0, sCnt0, slot0, sh0);
+                scan(sCnt0, pre0, total0);
+
                 // Two target chunks (up to 64 targets) share every staged window.
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
                 {
@@ -741,48 +764,71 @@ namespace sph
                     initChunk(Bc, rec, tc + 32, tEnd, lane);
                     for(int page = 0; page * 32 < nDesc; ++page)
                     {
-                    uint32_t sBeg, sCnt, slotD;
-                    T sh[3];
-                    describe(page * 32 + lane, sBeg, sCnt, slotD, sh);
-                    int const nsl = min(32, nDesc - page * 32);
-                    uint32_t incl = sCnt;
-#pragma unroll
-                    for(int d = 1; d < 32; d <<= 1)
+                    uint32_t sBeg = sBeg0, sCnt = sCnt0, slotD = slot0, pre = pre0, total = total0;
+                    T sh[3] = {sh0[0], sh0[1], sh0[2]};
+                    if(page > 0)
                     {
-                        uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
-                        if(lane >= d)
-                            incl += o;
+                        describe(page * 32 + lane, sBeg, sCnt, slotD, sh);
+                        scan(sCnt, pre, total);
                     }
-                    uint32_t const pre = incl - sCnt;
-                    uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
                     int const selfLane = selfDesc - page * 32;
+                    // entry of staged position q: eBase of q's descriptor + (q << 5)
+                    // (j = sBeg + q - pre, packed as (j << 5) | slot)
+                    uint32_t const eBase = ((sBeg - pre) << 5) | slotD;
                     for(uint32_t cb = 0; cb < total; cb += CAP)
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
                         __syncwarp();
-                        for(int sl = 0; sl < nsl; ++sl)
+                        // Flat staging: lane l fills window positions l, l + 32, ...; the
+                        // descriptor of position q is the last one whose prefix is <= q
+                        // (a shuffle binary search over the page's prefixes; empty
+                        // descriptors share the next one's prefix and are passed over).
+                        // kStageBatch positions' records are in flight at once.
+                        constexpr int KB = PairCfg<T>::kStageBatch;
+#pragma unroll 1
+                        for(uint32_t k0 = 0; cb + 32u * k0 < ce; k0 += KB)
                         {
-                            uint32_t const p0 = __shfl_sync(0xffffffffu, pre, sl);
-                            uint32_t const n0 = __shfl_sync(0xffffffffu, sCnt, sl);
-                            if(p0 + n0 <= cb || p0 >= ce)
-                                continue; // uniform: descriptor outside this window
-                            uint32_t const b0 = __shfl_sync(0xffffffffu, sBeg, sl);
-                            uint32_t const slotS = __shfl_sync(0xffffffffu, slotD, sl);
-                            T const sx = __shfl_sync(0xffffffffu, sh[0], sl);
-                            T const sy = __shfl_sync(0xffffffffu, sh[1], sl);
-                            T const sz = __shfl_sync(0xffffffffu, sh[2], sl);
-                            uint32_t const lo = max(p0, cb);
-                            uint32_t const hi2 = min(p0 + n0, ce);
-                            for(uint32_t q = lo + uint32_t(lane); q < hi2; q += 32)
+                            uint32_t ent[KB];
+                            int dsc[KB];
+                            V4 pj[KB];
+                            T hj[KB];
+#pragma unroll
+                            for(int k = 0; k < KB; ++k)
                             {
-                                uint32_t const j = b0 + (q - p0);
-                                V4 const pj = ld4(rec.pm + j);
-                                sNX[q - cb] = -addRn(pj.x, sx);
-                                sNY[q - cb] = -addRn(pj.y, sy);
-                                sNZ[q - cb] = -addRn(pj.z, sz);
-                                sEnt[q - cb] = packEntry(j, slotS);
-                                if constexpr(PAIRMAX)
-                                    sH[q - cb] = rec.hc[j];
+                                uint32_t const q = cb + uint32_t(lane) + 32u * (k0 + uint32_t(k));
+                                int sd = 0;
+#pragma unroll
+                                for(int step = 16; step >= 1; step >>= 1)
+                                {
+                                    uint32_t const v = __shfl_sync(0xffffffffu, pre, sd + step);
+                                    if(v <= q)
+                                        sd += step;
+                                }
+                                dsc[k] = sd;
+                                ent[k] = __shfl_sync(0xffffffffu, eBase, sd) + (q << 5);
+                                if(q < ce)
+                                {
+                                    pj[k] = ld4(rec.pm + (ent[k] >> 5));
+                                    if constexpr(PAIRMAX)
+                                        hj[k] = rec.hc[ent[k] >> 5];
+                                }
+                            }
+#pragma unroll
+                            for(int k = 0; k < KB; ++k)
+                            {
+                                uint32_t const w = uint32_t(lane) + 32u * (k0 + uint32_t(k));
+                                T const sx = __shfl_sync(0xffffffffu, sh[0], dsc[k]);
+                                T const sy = __shfl_sync(0xffffffffu, sh[1], dsc[k]);
+                                T const sz = __shfl_sync(0xffffffffu, sh[2], dsc[k]);
+                                if(cb + w < ce)
+                                {
+                                    sNX[w] = -addRn(pj[k].x, sx);
+                                    sNY[w] = -addRn(pj[k].y, sy);
+                                    sNZ[w] = -addRn(pj[k].z, sz);
+                                    sEnt[w] = ent[k];
+                                    if constexpr(PAIRMAX)
+                                        sH[w] = hj[k];
+                                }
                             }
                         }
                         uint32_t const m = ce - cb;
