@@ -234,7 +234,7 @@ namespace sph
         template<bool PAIRMAX>
         __device__ __forceinline__ uint32_t cullMask32(
             float4 const& own,
-            float hi,
+            float nRi2,
             float const* X,
             float const* Y,
             float const* Z,
@@ -266,12 +266,10 @@ namespace sph
                     float2 nr = nR2;
                     if constexpr(PAIRMAX)
                     {
-                        float const h0 = p ? hv.z : hv.x, h1 = p ? hv.w : hv.y;
-                        float2 const R = __fmul2_rn(
-                            make_float2(supT, supT),
-                            make_float2(hi > h0 ? hi : h0, hi > h1 ? hi : h1));
-                        float2 const RR = __fmul2_rn(R, R);
-                        nr = make_float2(-RR.x, -RR.y);
+                        // -(supT max(h_i, h_j))^2 = min(-(supT h_i)^2, -(supT h_j)^2):
+                        // the rounded product and square are monotone in h
+                        float const n0 = p ? hv.z : hv.x, n1 = p ? hv.w : hv.y;
+                        nr = make_float2(fminf(nRi2, n0), fminf(nRi2, n1));
                     }
                     float2 const d = __fadd2_rn(r2, nr);
                     mask = __funnelshift_l(__float_as_uint(d.x), mask, 1);
@@ -284,7 +282,7 @@ namespace sph
         template<bool PAIRMAX>
         __device__ __forceinline__ uint32_t cullMask32(
             D4 const& own,
-            double hi,
+            double nRi2,
             double const* X,
             double const* Y,
             double const* Z,
@@ -306,14 +304,10 @@ namespace sph
                     double const dy = __dadd_rn(own.y, p ? yv.y : yv.x);
                     double const dz = __dadd_rn(own.z, p ? zv.y : zv.x);
                     double const r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                    double R2 = R2g;
+                    double nR2 = -R2g;
                     if constexpr(PAIRMAX)
-                    {
-                        double const hj = H[q + p];
-                        double const R = __dmul_rn(supT, hi > hj ? hi : hj);
-                        R2 = __dmul_rn(R, R);
-                    }
-                    double const d = __dsub_rn(r2, R2);
+                        nR2 = fmin(nRi2, H[q + p]);
+                    double const d = __dadd_rn(r2, nR2);
                     mask = __funnelshift_l(uint32_t(__double2hiint(d)), mask, 1);
                 }
             }
@@ -326,6 +320,7 @@ namespace sph
         {
             V4 own;
             T hi;
+            T nR2;             //!< -(supT h_i)^2, the target's side of the pair-max cull radius
             uint32_t t;        //!< sorted target index
             uint32_t nl;       //!< accepted so far (same on every lane of the target's group)
             uint4 buf;         //!< full chunks: the last (nl mod 4) accepted entries, newest in w
@@ -340,7 +335,8 @@ namespace sph
             Records<V4, T> const& rec,
             uint32_t tc,
             uint32_t tEnd,
-            int lane)
+            int lane,
+            T supT)
         {
             uint32_t const nt = tc < tEnd ? min(32u, tEnd - tc) : 0u;
             ch.S = subLanes(nt == 0 ? 32u : nt);
@@ -360,6 +356,8 @@ namespace sph
                 ch.own = ld4(rec.pm + ch.t);
                 ch.hi = rec.hc[ch.t];
             }
+            T const Ri = mulRn(supT, ch.hi);
+            ch.nR2 = -mulRn(Ri, Ri);
         }
 
         //! Cull the staged candidates [0, m) against one target chunk and append
@@ -395,7 +393,7 @@ namespace sph
                 for(uint32_t q0 = 0; q0 < m; q0 += 32)
                 {
                     uint32_t mask
-                        = cullMask32<PAIRMAX>(ch.own, ch.hi, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
+                        = cullMask32<PAIRMAX>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
                     uint32_t const rel = mySelf - q0;
                     if(rel < 32u)
                         mask &= ~(0x80000000u >> rel);
@@ -441,11 +439,7 @@ namespace sph
                     T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
                     T R2 = R2g;
                     if constexpr(PAIRMAX)
-                    {
-                        T const hj = sH[qq];
-                        T const R = mulRn(supT, ch.hi > hj ? ch.hi : hj);
-                        R2 = mulRn(R, R);
-                    }
+                        R2 = -(ch.nR2 < sH[qq] ? ch.nR2 : sH[qq]);
                     entU[u] = sEnt[qq];
                     accU[u] = ok && r2 < R2 && entU[u] != selfEnt;
                 }
@@ -616,7 +610,7 @@ namespace sph
             T* const sNX = reinterpret_cast<T*>(smem) + warp * CAP;
             T* const sNY = sNX + kDensWarps * CAP;
             T* const sNZ = sNY + kDensWarps * CAP;
-            T* const sH = sNZ + kDensWarps * CAP; // only with PAIRMAX
+            T* const sH = sNZ + kDensWarps * CAP; // only with PAIRMAX: -(supT h_j)^2
             uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
                                    + warp * CAP;
             Records<V4, T> const rec = records<T>(c);
@@ -759,9 +753,9 @@ namespace sph
                 for(uint32_t tc = tBeg; tc < tEnd; tc += 64)
                 {
                     TargetChunk<V4, T> A, Bc;
-                    initChunk(A, rec, tc, tEnd, lane);
+                    initChunk(A, rec, tc, tEnd, lane, supT);
                     bool const twoChunks = tc + 32 < tEnd;
-                    initChunk(Bc, rec, tc + 32, tEnd, lane);
+                    initChunk(Bc, rec, tc + 32, tEnd, lane, supT);
                     for(int page = 0; page * 32 < nDesc; ++page)
                     {
                     uint32_t sBeg = sBeg0, sCnt = sCnt0, slotD = slot0, pre = pre0, total = total0;
@@ -827,7 +821,10 @@ namespace sph
                                     sNZ[w] = -addRn(pj[k].z, sz);
                                     sEnt[w] = ent[k];
                                     if constexpr(PAIRMAX)
-                                        sH[w] = hj[k];
+                                    {
+                                        T const Rj = mulRn(supT, hj[k]);
+                                        sH[w] = -mulRn(Rj, Rj);
+                                    }
                                 }
                             }
                         }
