@@ -176,6 +176,10 @@ struct sph_ctx
     int parity = 0;
     std::vector<cudaEvent_t> events;
     cudaEvent_t eCall = nullptr; //!< start of a step call (before its snapshot)
+    // Host<->device column copies run on their own stream so the copy engine
+    // works while the gather / unpermute kernels of other columns run.
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t eCopy = nullptr, eCompute = nullptr;
     double timings[5] = {0, 0, 0, 0, 0};
     // State a step call starts from, restored when a neighbour list overflowed
     // in any of its steps: the call then regrows the lists and runs again.
@@ -193,8 +197,26 @@ struct sph_ctx
             cudaEventDestroy(e);
         if(eCall)
             cudaEventDestroy(eCall);
+        if(eCopy)
+            cudaEventDestroy(eCopy);
+        if(eCompute)
+            cudaEventDestroy(eCompute);
+        if(copyStream)
+            cudaStreamDestroy(copyStream);
         if(stream)
             cudaStreamDestroy(stream);
+    }
+
+    //! The copy stream and its two hand-off events, created on first use.
+    int ensureCopyStream()
+    {
+        if(!copyStream)
+            SPH_CUDA_TRY(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+        if(!eCopy)
+            SPH_CUDA_TRY(cudaEventCreateWithFlags(&eCopy, cudaEventDisableTiming));
+        if(!eCompute)
+            SPH_CUDA_TRY(cudaEventCreateWithFlags(&eCompute, cudaEventDisableTiming));
+        return SPH_OK;
     }
 
     void dropGraphs()
@@ -1051,16 +1073,26 @@ int sph_ctx::setSpeciesFast(int32_t id, SphSoAView const* v)
 {
     HostSpecies& s = sp[id];
     int st = stagingCols(kHostCols);
-    if(st)
+    if(st || (st = ensureCopyStream()))
         return st;
     // h and source masses are checked on the device as they are gathered
     SPH_CUDA_TRY(cudaMemsetAsync(dc.status + sph::kStatBadInput, 0, sizeof(uint32_t), stream));
+    // Column c's copy (copy stream) hands over to its gather (context stream)
+    // through eCopy, so copy c + 1 runs under gather c.  The copies start after
+    // everything already queued on the context's stream.
+    SPH_CUDA_TRY(cudaEventRecord(eCompute, stream));
+    SPH_CUDA_TRY(cudaStreamWaitEvent(copyStream, eCompute, 0));
     for(int c = 0; c < kHostCols; ++c)
     {
         double const* src = viewCol(v, c);
         double* stage = staging[c];
         if(src)
-            SPH_CUDA_TRY(cudaMemcpyAsync(stage + s.offset, src, size_t(s.n) * 8, cudaMemcpyHostToDevice, stream));
+        {
+            SPH_CUDA_TRY(
+                cudaMemcpyAsync(stage + s.offset, src, size_t(s.n) * 8, cudaMemcpyHostToDevice, copyStream));
+            SPH_CUDA_TRY(cudaEventRecord(eCopy, copyStream));
+            SPH_CUDA_TRY(cudaStreamWaitEvent(stream, eCopy, 0));
+        }
         bool const mustBePositive = c == cH || (c == cM && (s.roles & SPH_ROLE_SOURCE));
         sph::launchGatherSpecies(
             n,
@@ -1338,8 +1370,10 @@ int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* v)
     size_t k = 0;
     for(auto const& c : cols)
         k += c.second ? 1 : 0;
-    if((st = ctx->stagingCols(k + 1)))
+    if((st = ctx->stagingCols(k + 1)) || (st = ctx->ensureCopyStream()))
         return st;
+    // Column k's unpermute (context stream) hands over to its copy (copy
+    // stream) through eCompute, so copy k runs under unpermute k + 1.
     k = 0;
     for(auto const& c : cols)
     {
@@ -1347,14 +1381,22 @@ int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* v)
             continue;
         double* stage = ctx->staging[k++];
         sph::launchUnpermute(ctx->n, d.cur.id, c.first, stage, ctx->stream);
-        SPH_CUDA_TRY(cudaMemcpyAsync(c.second, stage + s.offset, size_t(s.n) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaEventRecord(ctx->eCompute, ctx->stream));
+        SPH_CUDA_TRY(cudaStreamWaitEvent(ctx->copyStream, ctx->eCompute, 0));
+        SPH_CUDA_TRY(
+            cudaMemcpyAsync(c.second, stage + s.offset, size_t(s.n) * 8, cudaMemcpyDeviceToHost, ctx->copyStream));
     }
     if(v->box_id)
     {
         int32_t* istage = reinterpret_cast<int32_t*>(ctx->staging[k]);
         sph::launchUnpermuteInt(ctx->n, d.cur.id, reinterpret_cast<uint32_t const*>(d.cur.box), istage, ctx->stream);
-        SPH_CUDA_TRY(cudaMemcpyAsync(v->box_id, istage + s.offset, size_t(s.n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        SPH_CUDA_TRY(cudaEventRecord(ctx->eCompute, ctx->stream));
+        SPH_CUDA_TRY(cudaStreamWaitEvent(ctx->copyStream, ctx->eCompute, 0));
+        SPH_CUDA_TRY(
+            cudaMemcpyAsync(v->box_id, istage + s.offset, size_t(s.n) * 4, cudaMemcpyDeviceToHost, ctx->copyStream));
     }
+    // every unpermute precedes a copy the copy stream waited for
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->copyStream));
     SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return SPH_OK;
 }
