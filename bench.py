@@ -245,6 +245,17 @@ def traffic_from_profiles(name):
     return None
 
 
+def hbm_view(kernel, peak_gbs):
+    """A pair kernel's DRAM traffic per launch over its event-timed launch, as a
+    fraction of the measured HBM copy bandwidth (None without an ncu capture)."""
+    traffic, ms = kernel.get("traffic"), kernel.get("ms_per_launch")
+    if not traffic or not ms or not peak_gbs:
+        return None
+    gbs = traffic / (ms * 1e-3) / 1e9
+    return {"achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": gbs / peak_gbs,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+
+
 def measured_peak(key):
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get(key)
@@ -488,7 +499,10 @@ def run_ours(args, rank, world):
                          "pairs_per_launch": pairs_step,
                          "peak_source": "measured live (FMA-chain microbenchmark, sphx_fma_tflops)",
                          "other_pair_kernel": other,
-                         "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs")},
+                         "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs"),
+                         # the same launch against HBM: ncu DRAM bytes per launch (profiles/)
+                         # over the event-timed launch, of the measured copy bandwidth
+                         "hbm": hbm_view(dominant, measured_peak("hbm_gbs"))},
             "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(launches),

@@ -43,3 +43,10 @@ def test_flop_constants():
     assert flops.PASSES_PER_STEP["mhd"] == 3
     assert flops.FORCE_FLOPS["mhd"] > flops.FORCE_FLOPS["hydro"] > flops.DENSITY_FLOPS["cubic"]
     assert flops.CULL_FLOPS_PER_CANDIDATE == 9
+
+
+def test_hbm_view_of_a_launch():
+    v = bench.hbm_view({"traffic": 6.5e8, "ms_per_launch": 1.0}, 6500.0)
+    assert v["unit"] == "GB/s" and abs(v["achieved"] - 650.0) < 1e-9 and abs(v["frac"] - 0.1) < 1e-12
+    assert bench.hbm_view({"traffic": None, "ms_per_launch": 1.0}, 6500.0) is None
+    assert bench.hbm_view({"traffic": 6.5e8, "ms_per_launch": 1.0}, None) is None
