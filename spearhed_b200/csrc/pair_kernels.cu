@@ -40,14 +40,12 @@ namespace sph
         struct PairCfg<float>
         {
             using V4 = float4;
-            static constexpr int cap = 256;
             static constexpr int kStageBatch = 2; //!< staged positions per lane with loads in flight
         };
         template<>
         struct PairCfg<double>
         {
             using V4 = D4;
-            static constexpr int cap = 256;
             static constexpr int kStageBatch = 2;
         };
 
