@@ -506,6 +506,9 @@ def run_ours(args, rank, world):
             "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(launches),
+            # step calls re-run after a neighbour-list overflow inside the timed region
+            # (a replay's first attempt is in the time, not in the pair count)
+            "list_replays_timed": int(d1["replays"] - d0["replays"]),
             "clocks": clk.summary(),
         }
         if cpu is not None:

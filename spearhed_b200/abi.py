@@ -104,6 +104,8 @@ class SphDiag(C.Structure):
         ("n_targets", C.c_int64),
         ("pairs_total", C.c_double),
         ("candidates", C.c_double),
+        ("replays", C.c_int64),
+        ("list_capacity", C.c_int64),
     ]
 
     def as_dict(self):

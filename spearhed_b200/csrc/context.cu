@@ -184,6 +184,9 @@ struct sph_ctx
     // State a step call starts from, restored when a neighbour list overflowed
     // in any of its steps: the call then regrows the lists and runs again.
     int densityVariant = 0, forceVariant = 0; //!< launch shapes (sph_autotune / sph_set_tuning)
+    int64_t replays = 0;                      //!< step calls re-run after a list overflow
+    bool anyTwoLevel = false;                 //!< some box allocates level-1 cells
+    uint32_t lastStat[sph::kStatWords] = {};  //!< status words of the last checkStatus
     SphTuning tuning{};
     bool haveSnap = false;
     sph::Master snap{};
@@ -456,10 +459,12 @@ int sph_ctx::layout()
                 hmax[b] = std::max(hmax[b], s.col[cH][i]);
                 hmin[b] = std::min(hmin[b], s.col[cH][i]);
             }
+
         }
     }
     boxDesc.assign(nbox, sph::BoxDev{});
     uint64_t cellBase = 0, activeBase = 0;
+    anyTwoLevel = false;
     bool const dynamic = p.cull == SPH_CULL_PAIR_MAX;
     for(int32_t b = 0; b < nbox; ++b)
     {
@@ -470,7 +475,15 @@ int sph_ctx::layout()
         double const hgrid = hmax[b];
         if(dynamic && p.h_max > 0.0 && p.h_max < hmax[b])
             return fail(SPH_ERR_INVALID, "an input h exceeds params.h_max");
-        double const rc = cellRadius(sup, hgrid);
+        // Boxes whose h spans a factor of 1.6 or more also allocate level-1 cells
+        // (m0 x m1 x m2 per level-0 cell, each m in 1..4) for the particles whose
+        // cull radius fits a level-1 edge; the grid update decides each step
+        // whether they are used and how finely, with the level-0 edge covering
+        // both the largest radius and twice the smallest.
+        bool const two = dynamic && hmin[b] < 1e300
+                         && 2.0 * cellRadius(sup, hmin[b]) <= sph::kTwoLevelSlack * cellRadius(sup, hgrid);
+        double const rc = two ? std::max(cellRadius(sup, hgrid), 2.0 * cellRadius(sup, hmin[b])) : cellRadius(sup, hgrid);
+        double const rAlloc = cellRadius(sup, hgrid);
         sph::BoxDev& d = boxDesc[b];
         uint64_t cells = 1, cellsMax = 1;
         // adaptive h is capped by h_max, else by what the periodic axes admit
@@ -484,11 +497,11 @@ int sph_ctx::layout()
             d.periodic[a] = B.periodic[a] ? 1 : 0;
             double const nd = std::floor(d.L[a] / rc);
             d.n[a] = nd < 1.0 ? 1 : (nd > 1.0e6 ? 1000000 : int32_t(nd));
-            double const ndMax = dynamic ? std::floor(d.L[a] / (0.5 * rc)) : nd;
+            double const ndMax = dynamic ? std::floor(d.L[a] / (0.5 * rAlloc)) : nd;
             d.nMax[a] = std::max(d.n[a], ndMax < 1.0 ? 1 : (ndMax > 1.0e6 ? 1000000 : int32_t(ndMax)));
             d.edge[a] = d.L[a] / d.n[a];
             d.edgef[a] = float(d.edge[a]);
-            if(d.periodic[a] && d.L[a] < rc)
+            if(d.periodic[a] && d.L[a] < rAlloc)
                 return fail(SPH_ERR_UNSUPPORTED, "periodic box thinner than the interaction radius");
             if(d.periodic[a] && p.h_max <= 0.0 && (p.physics & SPH_PHYS_ADAPTIVE_H))
             {
@@ -500,19 +513,23 @@ int sph_ctx::layout()
             cells *= uint64_t(d.n[a]);
             cellsMax *= uint64_t(d.nMax[a]);
         }
-        // Boxes whose h spans a factor of two or more also allocate level-1 cells
-        // (2x2x2 per level-0 cell) for the particles whose cull radius fits half
-        // a cell; the grid update decides each step whether they are used.
-        d.levelsAlloc = dynamic && hmin[b] <= 0.5 * hmax[b] ? 2 : 1;
-        d.e1 = 0.5 * std::min(d.edge[0], std::min(d.edge[1], d.edge[2]));
-        d.levels = d.levelsAlloc == 2 && cellRadius(sup, hmin[b]) <= d.e1 ? 2 : 1;
+        // Level-1 cells: up to 2 x 2 x 2 per allocated level-0 cell.  The grid
+        // update chooses the splits each step; until it runs the box has one level.
+        d.levelsAlloc = two ? 2 : 1;
+        uint64_t const perCell = two ? 8 : 0;
+        d.cells1Alloc = uint32_t(perCell * cellsMax);
+        d.levels = 1;
+        d.m[0] = d.m[1] = d.m[2] = 1;
+        d.msub = 1;
+        d.e1 = 0.0;
         d.cellBase = uint32_t(cellBase);
         d.ncells = uint32_t(cells);
         d.ncellsMax = uint32_t(cellsMax);
-        d.nItems = uint32_t(d.levels == 2 ? 9 * cells : cells);
+        d.nItems = uint32_t(cells);
         d.activeBase = uint32_t(activeBase);
         d.hcap = hcap;
-        cellBase += d.levelsAlloc == 2 ? 9 * cellsMax : cellsMax;
+        cellBase += cellsMax + perCell * cellsMax;
+        anyTwoLevel = anyTwoLevel || two;
         activeBase += d.nItems;
         if(cellBase * 2 + 1 >= (1ull << 32))
             return fail(SPH_ERR_UNSUPPORTED, "too many cells (2^31)");
@@ -553,7 +570,8 @@ int sph_ctx::allocate()
             return st;
     }
     dc.cells.ncells = ncells;
-    if((st = alloc(dc.cells.start, ncells)) || (st = alloc(dc.cells.mid, ncells)) || (st = alloc(dc.cells.end, ncells)))
+    if((st = alloc(dc.cells.start, ncells)) || (st = alloc(dc.cells.mid, ncells)) || (st = alloc(dc.cells.end, ncells))
+       || (st = alloc(dc.cells.bstart, ncells)) || (st = alloc(dc.cells.bend, ncells)))
         return st;
     if((st = alloc(dc.keysA, n)) || (st = alloc(dc.valsA, n)) || (st = alloc(dc.keysB, n)) || (st = alloc(dc.valsB, n))
        || (st = alloc(dc.sortScratch, sph::radixScratchWords(n))))
@@ -751,6 +769,8 @@ int sph_ctx::build(bool drift)
     uint32_t const* keys = inB ? dc.keysB : dc.keysA;
     uint32_t const* perm = inB ? dc.valsB : dc.valsA;
     sph::launchCellRanges(dc, keys, stream);
+    if(anyTwoLevel)
+        sph::launchSubBlocks(dc, ncells, stream);
     sph::launchPermute(dc, perm, pa, p.precision, stream);
     std::swap(dc.cur, dc.alt);
     parity ^= 1;
@@ -819,8 +839,8 @@ int sph_ctx::snapshot(bool restore)
 
 int sph_ctx::checkStatus(char const* where)
 {
-    uint32_t stat[sph::kStatWords];
-    SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost, stream));
+    uint32_t* const stat = lastStat;
+    SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(lastStat), cudaMemcpyDeviceToHost, stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
     SPH_CUDA_TRY(cudaGetLastError());
     if(stat[sph::kStatNonFinite])
@@ -897,6 +917,7 @@ int sph_ctx::steps(int32_t nsteps, double dt)
         }
         if(st != SPH_ERR_OVERFLOW)
             break;
+        ++replays;
         uint32_t stat[sph::kStatWords];
         SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
         int const g = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16);
@@ -910,6 +931,18 @@ int sph_ctx::steps(int32_t nsteps, double dt)
         timings[4] = ms;
     densityValid = st == SPH_OK;
     forceValid = st == SPH_OK;
+    // Headroom: a call whose largest list came within 10% of the capacity grows
+    // the lists now (after its timed events), so slowly rising neighbour counts
+    // do not make a later call overflow and run again.  The derivatives stay
+    // valid; the lists of this state are gone, so the density pass is not.
+    uint32_t const maxCount = lastStat[sph::kStatMaxCount];
+    if(st == SPH_OK && uint64_t(maxCount) * 10 > uint64_t(dc.lists.cap) * 9)
+    {
+        int const g = growLists(uint32_t(double(maxCount) * 1.25) + 16);
+        if(g)
+            return g;
+        forceValid = true;
+    }
     return st;
 }
 
@@ -1494,6 +1527,8 @@ int sph_reduce(sph_ctx* ctx, SphDiag* out)
         }
     *out = SphDiag{};
     fillDiag(*out, a, sc, hb, 0);
+    out->replays = ctx->replays;
+    out->list_capacity = ctx->dc.lists.cap;
     // an ensemble reports the largest c_h and the smallest next dt over its boxes
     for(uint32_t b = 1; b < ctx->dc.nbox; ++b)
     {
@@ -1520,6 +1555,8 @@ int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
     {
         out[b] = SphDiag{};
         fillDiag(out[b], &pb[size_t(b) * sph::kDiagWords], sc, hb, uint32_t(b));
+        out[b].replays = ctx->replays;
+        out[b].list_capacity = ctx->dc.lists.cap;
     }
     return SPH_OK;
 }

@@ -653,25 +653,34 @@ namespace sph
                     chBox = box;
                 }
                 BoxDev const& B = c.boxes[box];
-                // Target cell: level 0 (the grid) or level 1 (the 2x2x2 sub-cells of
-                // a level-0 cell), its coordinates in its level and its level-0 parent.
+                // Target cell: level 0 (the grid) or level 1 (one of the m0 x m1 x m2
+                // sub-cells of a level-0 cell, numbered parent-major), its level-0
+                // parent c0 and, for level 1, its coordinates ct on the fine grid
+                // (m_a n_a cells per axis).
                 int const lt = l < B.ncells ? 0 : 1;
                 int ct[3], c0[3];
                 {
                     uint32_t const li = lt ? l - B.ncells : l;
-                    uint32_t const n0 = uint32_t(B.n[0]) << lt, n1 = uint32_t(B.n[1]) << lt;
-                    ct[0] = int(li % n0);
-                    ct[1] = int((li / n0) % n1);
-                    ct[2] = int(li / (n0 * n1));
+                    uint32_t const par = lt ? li / B.msub : li;
+                    uint32_t const n0 = uint32_t(B.n[0]), n1 = uint32_t(B.n[1]);
+                    c0[0] = int(par % n0);
+                    c0[1] = int((par / n0) % n1);
+                    c0[2] = int(par / (n0 * n1));
+                    uint32_t sub = lt ? li - par * B.msub : 0u;
 #pragma unroll
                     for(int a = 0; a < 3; ++a)
-                        c0[a] = ct[a] >> lt;
+                    {
+                        uint32_t const sh = uint32_t(B.m[a] - 1); // splits are 1 or 2
+                        ct[a] = (c0[a] << sh) + int(sub & sh);
+                        sub >>= sh;
+                    }
                 }
                 // Candidate descriptors: the 27 level-0 cells around the parent, then
-                // with two levels the 27 level-1 cells around a level-1 target or the
-                // 216 level-1 sub-cells of those 27 cells for a level-0 target.  Each
-                // carries its source range and the level-0 stencil slot of its image.
-                int const nDesc = 27 + (B.levels == 2 ? (lt ? 27 : 216) : 0);
+                // with two levels either the 27 level-1 cells around a level-1 target
+                // or, for a level-0 target, the level-1 block (all sub-cells) of each
+                // of those 27 cells.  Each carries its source range and the level-0
+                // stencil slot of its image.
+                int const nDesc = 27 + (B.levels == 2 ? 27 : 0);
                 int const selfDesc = lt ? 27 + kCentreSlot : kCentreSlot;
                 auto describe = [&](int d, uint32_t& sBeg, uint32_t& sCnt, uint32_t& slot, T sh[3])
                 {
@@ -684,24 +693,25 @@ namespace sph
                     int o[3], f[3];
                     bool ok = true;
                     bool const fine = d >= 27;
-                    int const k = d - 27;
-                    int const on = d < 27 ? d : (lt ? 0 : (k >> 3)); // level-0 neighbour of the coarse paths
+                    int const k = fine ? d - 27 : d;
+                    bool const fineCell = fine && lt; // a level-1 neighbour of a level-1 target
 #pragma unroll
                     for(int a = 0; a < 3; ++a)
                     {
                         int const n0 = B.n[a];
-                        if(fine && lt)
+                        if(fineCell)
                         {
-                            // level-1 neighbour of a level-1 target
+                            // fine-grid neighbour; its level-0 parent (image-aware) gives o
+                            int const sh = B.m[a] - 1; // splits are 1 or 2
+                            int const n1 = n0 << sh;
                             int const fa = ct[a] + stencilOff(k, a);
-                            o[a] = (fa >> 1) - c0[a];
-                            int const n1 = 2 * n0;
+                            o[a] = (fa >> sh) - c0[a];
                             f[a] = fa < 0 || fa >= n1 ? (B.periodic[a] ? (fa + n1) % n1 : -1) : fa;
                             ok = ok && f[a] >= 0;
                         }
                         else
                         {
-                            o[a] = stencilOff(on, a);
+                            o[a] = stencilOff(k, a);
                             int ca = c0[a] + o[a];
                             if(ca < 0 || ca >= n0)
                             {
@@ -710,7 +720,7 @@ namespace sph
                                 else
                                     ok = false;
                             }
-                            f[a] = fine ? 2 * ca + ((k >> a) & 1) : ca; // sub-cell k & 7 of a level-0 neighbour
+                            f[a] = ca;
                         }
                     }
                     slot = uint32_t((o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1));
@@ -719,11 +729,38 @@ namespace sph
                         sh[a] = T(o[a]) * edgeOf<T>(B, a);
                     if(!ok)
                         return;
-                    uint32_t const m0 = uint32_t(B.n[0]) << (fine ? 1 : 0), m1 = uint32_t(B.n[1]) << (fine ? 1 : 0);
-                    uint32_t const idx = (uint32_t(f[2]) * m1 + uint32_t(f[1])) * m0 + uint32_t(f[0]);
-                    uint32_t const cellId = B.cellBase + (fine ? B.ncellsMax : 0u) + idx;
-                    sBeg = c.cells.start[cellId];
-                    sCnt = c.cells.end[cellId] - sBeg;
+                    if(fineCell)
+                    {
+                        int p[3];
+                        uint32_t subc = 0, stride = 1;
+#pragma unroll
+                        for(int a = 0; a < 3; ++a)
+                        {
+                            int const sh = B.m[a] - 1;
+                            p[a] = f[a] >> sh;
+                            subc += uint32_t(f[a] & sh) * stride;
+                            stride <<= sh;
+                        }
+                        uint32_t const par = (uint32_t(p[2]) * uint32_t(B.n[1]) + uint32_t(p[1])) * uint32_t(B.n[0])
+                                             + uint32_t(p[0]);
+                        uint32_t const cellId = B.cellBase + B.ncellsMax + par * B.msub + subc;
+                        sBeg = c.cells.start[cellId];
+                        sCnt = c.cells.end[cellId] - sBeg;
+                        return;
+                    }
+                    uint32_t const cellId
+                        = B.cellBase + (uint32_t(f[2]) * uint32_t(B.n[1]) + uint32_t(f[1])) * uint32_t(B.n[0]) + uint32_t(f[0]);
+                    if(fine)
+                    {
+                        // all level-1 sub-cells of a level-0 neighbour, as one range
+                        sBeg = c.cells.bstart[cellId];
+                        sCnt = c.cells.bend[cellId] - sBeg;
+                    }
+                    else
+                    {
+                        sBeg = c.cells.start[cellId];
+                        sCnt = c.cells.end[cellId] - sBeg;
+                    }
                 };
 
                 // exclusive prefix of the page's source counts and the page total

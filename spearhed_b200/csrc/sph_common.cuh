@@ -25,12 +25,15 @@ namespace sph
         uint32_t ncells;   //!< cells of the current grid (n[0] n[1] n[2])
         double hcap;       //!< cap on adaptive h (params.h_max, else what the periodic axes admit)
         int32_t nMax[3];   //!< allocated cells per axis: the current grid never exceeds them
-        uint32_t ncellsMax; //!< allocated level-0 cells; level-1 cells (8 per level-0 cell) follow them
+        uint32_t ncellsMax; //!< allocated level-0 cells; the cells1Alloc level-1 cells follow them
         uint32_t activeBase; //!< first work item of this box (prefix of items over boxes)
-        uint32_t nItems;     //!< work items: ncells, times 9 with two levels
+        uint32_t nItems;     //!< work items: ncells, plus ncells * msub with two levels
         int32_t levelsAlloc; //!< 2 when level-1 cells are allocated
         int32_t levels;      //!< 2 when this step bins small-h particles into level-1 cells
-        double e1;           //!< level-1 cell edge bound: a particle whose cell radius fits it is level 1
+        double e1;           //!< smallest level-1 edge: a particle whose cell radius fits it is level 1
+        int32_t m[3];        //!< level-1 sub-cells per level-0 cell along each axis (1 or 2)
+        uint32_t msub;       //!< m[0] m[1] m[2]; level-1 cell of level-0 cell l, sub-cell s: l * msub + s
+        uint32_t cells1Alloc; //!< allocated level-1 cells
     };
 
     //! Roles (include/spearhed_b200.h, SPH_ROLE_*).
@@ -78,6 +81,11 @@ namespace sph
     }
 
     //! A neighbour-list entry: sorted source index (27 bits) and stencil slot (5 bits).
+    //! A box runs two cell levels while twice its smallest cull radius is at
+    //! most this factor times its largest (h range >= 1.6); its level-0 edge
+    //! then covers both radii.
+    constexpr double kTwoLevelSlack = 1.25;
+
     __host__ __device__ __forceinline__ uint32_t packEntry(uint32_t j, uint32_t slot)
     {
         return (j << 5) | slot;

@@ -155,6 +155,10 @@ namespace sph
         uint32_t* mid;
         uint32_t* end;
         uint32_t ncells;
+        //! Two-level boxes: the sorted range of all level-1 sub-cells of level-0
+        //! cell c (contiguous, parent-major numbering), at the level-0 cell id.
+        uint32_t* bstart;
+        uint32_t* bend;
     };
 
     //! Neighbour lists: row t (sorted target index) holds count[t] entries of
@@ -328,6 +332,9 @@ namespace sph
     //! Grid of every box from its particles' current largest h (pair-max cull):
     //! n = floor(L / cellRadius(support, hmax)) clamped to [1, nMax], the
     //! stencil shift tables, the active-cell prefix and total.
+    //! Level-1 block range (bstart/bend) of every level-0 cell of the boxes
+    //! that run two levels this step; totalCells bounds the work items.
+    void launchSubBlocks(DevCtx const& c, uint32_t totalCells, cudaStream_t s);
     void launchGridUpdate(DevCtx const& c, int support, cudaStream_t s);
 
     //! dst <- src for every master column (n particles).

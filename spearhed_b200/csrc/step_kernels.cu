@@ -74,17 +74,19 @@ namespace sph
                                     + uint32_t(cc[0]);
                     if(B.levels == 2 && cellRadiusDev(c.support, c.cur.h[p]) <= B.e1)
                     {
-                        // level 1: the 2x2x2 sub-cell of the level-0 cell, from the
-                        // position relative to the cell corner (as the permute computes it)
-                        int f[3];
+                        // level 1: the sub-cell of the level-0 cell, from the position
+                        // relative to the cell corner (as the permute computes it);
+                        // sub-cells of one level-0 cell are numbered together
+                        uint32_t sub = 0, stride = 1;
 #pragma unroll
                         for(int a = 0; a < 3; ++a)
                         {
                             double const rel = x[a] - (B.lo[a] + double(cc[a]) * B.edge[a]);
-                            f[a] = 2 * cc[a] + (rel >= 0.5 * B.edge[a] ? 1 : 0);
+                            uint32_t const s = B.m[a] == 2 && rel >= 0.5 * B.edge[a] ? 1u : 0u;
+                            sub += s * stride;
+                            stride *= uint32_t(B.m[a]);
                         }
-                        uint32_t const m0 = 2u * uint32_t(B.n[0]), m1 = 2u * uint32_t(B.n[1]);
-                        cell = B.cellBase + B.ncellsMax + (uint32_t(f[2]) * m1 + uint32_t(f[1])) * m0 + uint32_t(f[0]);
+                        cell = B.cellBase + B.ncellsMax + (cell - B.cellBase) * B.msub + sub;
                     }
                     key = 2u * cell + (isTarget(role) ? 0u : 1u);
                 }
@@ -415,9 +417,17 @@ namespace sph
             {
                 BoxDev& B = c.boxes[b];
                 double const h = __longlong_as_double(static_cast<long long>(c.bs.hmaxBits[b]));
+                double const hmin = __longlong_as_double(static_cast<long long>(c.bs.hminBits[b]));
+                // Two levels pay once the smallest radius is under 1/1.6 of the
+                // largest: the level-0 edge then also covers twice the smallest
+                // radius (at most 1.25x the largest), so the small-h particles
+                // always fit a level-1 sub-cell, also when the range hovers at 2.
+                bool const two = B.levelsAlloc == 2 && h > 0.0 && hmin > 0.0 && hmin < 1e300
+                                 && 2.0 * cellRadiusDev(sup, hmin) <= kTwoLevelSlack * cellRadiusDev(sup, h);
                 if(h > 0.0)
                 {
-                    double const rc = cellRadiusDev(sup, h);
+                    double const rc = two ? fmax(cellRadiusDev(sup, h), 2.0 * cellRadiusDev(sup, hmin))
+                                          : cellRadiusDev(sup, h);
                     uint32_t cells = 1;
                     for(int a = 0; a < 3; ++a)
                     {
@@ -430,14 +440,40 @@ namespace sph
                     }
                     B.ncells = cells;
                 }
-                // two levels when the box allocates them and its smallest h fits half a cell
-                double e1 = 0.5 * B.edge[0];
-                e1 = fmin(e1, 0.5 * B.edge[1]);
-                e1 = fmin(e1, 0.5 * B.edge[2]);
+                // Level-1 split: halves on every axis whose edge holds twice the
+                // smallest cull radius (finer splits leave too few targets per
+                // sub-cell, and a split sized by the smallest h alone misses the
+                // bulk of the small-h particles); reduced until the sub-cells fit
+                // the allocation.  Two levels need at least two sub-cells.
+                int m[3] = {1, 1, 1};
+                if(two)
+                {
+                    double const rmin = cellRadiusDev(sup, hmin);
+                    for(int a = 0; a < 3; ++a)
+                        m[a] = B.edge[a] >= 2.0 * rmin ? 2 : 1;
+                    while(uint64_t(m[0] * m[1] * m[2]) * B.ncells > B.cells1Alloc && m[0] * m[1] * m[2] > 1)
+                    {
+                        int const a = (m[0] >= m[1] && m[0] >= m[2]) ? 0 : (m[1] >= m[2] ? 1 : 2);
+                        --m[a];
+                    }
+                }
+                uint32_t const msub = uint32_t(m[0] * m[1] * m[2]);
+                B.levels = two && msub >= 2 ? 2 : 1;
+                double e1 = 0.0;
+                if(B.levels == 2)
+                {
+                    e1 = B.edge[0] / double(m[0]);
+                    e1 = fmin(e1, B.edge[1] / double(m[1]));
+                    e1 = fmin(e1, B.edge[2] / double(m[2]));
+                }
+                else
+                    m[0] = m[1] = m[2] = 1;
+#pragma unroll
+                for(int a = 0; a < 3; ++a)
+                    B.m[a] = m[a];
+                B.msub = B.levels == 2 ? msub : 1u;
                 B.e1 = e1;
-                double const hmin = __longlong_as_double(static_cast<long long>(c.bs.hminBits[b]));
-                B.levels = (B.levelsAlloc == 2 && hmin > 0.0 && hmin < 1e300 && cellRadiusDev(sup, hmin) <= e1) ? 2 : 1;
-                B.nItems = B.levels == 2 ? 9u * B.ncells : B.ncells;
+                B.nItems = B.levels == 2 ? B.ncells * (1u + msub) : B.ncells;
                 for(int sl = 0; sl < 32; ++sl)
                 {
                     int const o[3] = {stencilOff(sl, 0), stencilOff(sl, 1), stencilOff(sl, 2)};
@@ -464,6 +500,35 @@ namespace sph
                 }
                 *c.activeTotal = base;
             }
+        }
+
+        //! Level-1 block range of each level-0 cell of a two-level box: the union
+        //! of its sub-cells' sorted ranges, which are contiguous because the
+        //! sub-cells of one level-0 cell are numbered together.  One thread per
+        //! work item; level-1 items and one-level boxes have nothing to do.
+        __global__ void __launch_bounds__(kThreads) kSubBlocks(DevCtx c)
+        {
+            uint32_t const q = blockIdx.x * blockDim.x + threadIdx.x;
+            if(q >= *c.activeTotal)
+                return;
+            int const box = boxOfWork(c.boxes, c.nbox, q);
+            BoxDev const& B = c.boxes[box];
+            uint32_t const l = q - B.activeBase;
+            if(B.levels != 2 || l >= B.ncells)
+                return;
+            uint32_t const first = B.cellBase + B.ncellsMax + l * B.msub;
+            uint32_t lo = 0xffffffffu, hi = 0;
+            for(uint32_t sc = 0; sc < B.msub; ++sc)
+            {
+                uint32_t const s = c.cells.start[first + sc], e = c.cells.end[first + sc];
+                if(e > s)
+                {
+                    lo = min(lo, s);
+                    hi = max(hi, e);
+                }
+            }
+            c.cells.bstart[B.cellBase + l] = hi > 0 ? lo : 0u;
+            c.cells.bend[B.cellBase + l] = hi;
         }
 
         //! Copy of every master column (the state a step call starts from).
@@ -729,6 +794,15 @@ namespace sph
         if(n)
         {
             kGatherSpeciesInt<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(n, id, off, cnt, src, master);
+            countLaunches(1);
+        }
+    }
+
+    void launchSubBlocks(DevCtx const& c, uint32_t totalCells, cudaStream_t s)
+    {
+        if(totalCells)
+        {
+            kSubBlocks<<<(totalCells + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
             countLaunches(1);
         }
     }

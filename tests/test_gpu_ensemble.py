@@ -124,3 +124,6 @@ def test_list_overflow_in_a_step_call_replays_from_its_start(prec):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
     assert dg["time"] == dref[0]["time"]
     assert dg["steps"] == dref[0]["steps"] == 5
+    # the call ran again once its lists had grown; the reference run never did
+    assert dg["replays"] >= 1 and dref[0]["replays"] == 0
+    assert dg["list_capacity"] > 32 and dref[0]["list_capacity"] == 256

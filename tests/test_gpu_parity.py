@@ -108,12 +108,13 @@ def test_two_particles_at_rest_repel(oracle, prec):
 
 
 # ---- random clouds: pair sets, density, forces ----------------------------
-def _cloud(kernel, prec, n=3000, seed=5, periodic=(0, 1, 1), physics=0, cull=abi.CULL_GLOBAL, vary_h=False):
+def _cloud(kernel, prec, n=3000, seed=5, periodic=(0, 1, 1), physics=0, cull=abi.CULL_GLOBAL, vary_h=False,
+           h_lo=0.6):
     rng = np.random.default_rng(seed)
     s = abi.Species(n)
     s.pos[:] = rng.uniform(0.0, 1.0, size=(3, n))
     h0 = 0.07 if kernel != QUINTIC else 0.05
-    s.h[:] = h0 * (rng.uniform(0.6, 1.0, n) if vary_h else 1.0)
+    s.h[:] = h0 * (rng.uniform(h_lo, 1.0, n) if vary_h else 1.0)
     s.mass[:] = rng.uniform(0.5, 1.5, n) * 1e-3
     s.u[:] = rng.uniform(0.5, 2.0, n)
     s.vel[:] = rng.normal(size=(3, n)) * 0.3
@@ -127,6 +128,26 @@ def _cloud(kernel, prec, n=3000, seed=5, periodic=(0, 1, 1), physics=0, cull=abi
 @pytest.mark.parametrize("cull,vary", [(abi.CULL_GLOBAL, False), (abi.CULL_PAIR_MAX, True)])
 def test_density_and_pairs_match_oracle(oracle, kernel, prec, cull, vary):
     p, boxes, sp = _cloud(kernel, prec, cull=cull, vary_h=vary)
+    ctx = _ctx(p, boxes, sp)
+    ctx.density()
+    got = ctx.get_species(abi.SPECIES_DEFAULT)
+    counts = ctx.neighbour_counts(abi.SPECIES_DEFAULT)
+    orc = _oracle(oracle, p, boxes, sp)
+    ocounts, _ = orc.neighbour_counts(fp32_geometry=(prec == abi.PREC_FP32_COMP))
+    assert np.array_equal(counts, ocounts)
+    orc.density()
+    rel = np.max(np.abs(got.density / orc.s.density - 1.0))
+    assert rel <= TOL[prec]["rho"], rel
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("h_lo,n", [(0.25, 6000), (0.4, 4000)])
+def test_two_level_grid_pairs_match_oracle(oracle, prec, h_lo, n):
+    """Smoothing lengths spanning 4x and 2.5x under the pair-max cull: the box
+    runs two cell levels with 3- or 4-way splits of the level-0 cells (the
+    oracle searches one level); the accepted pair sets are the same and the
+    densities agree to round-off."""
+    p, boxes, sp = _cloud(CUBIC, prec, n=n, cull=abi.CULL_PAIR_MAX, vary_h=True, h_lo=h_lo)
     ctx = _ctx(p, boxes, sp)
     ctx.density()
     got = ctx.get_species(abi.SPECIES_DEFAULT)
