@@ -370,7 +370,7 @@ struct sph_ctx
     int downloadMirror();
     int ensureDevice();
     int probeListCapacity();
-    int growLists(uint32_t need);
+    int growLists(uint32_t need, bool bestEffort = false);
     int build(bool drift);
     int clearStatus();
     int checkStatus(char const* where);
@@ -706,10 +706,22 @@ int sph_ctx::probeListCapacity()
 }
 
 //! (Re)allocates the neighbour lists with room for `need` entries per target.
-int sph_ctx::growLists(uint32_t need)
+int sph_ctx::growLists(uint32_t need, bool bestEffort)
 {
     uint32_t const capN = std::max<uint32_t>(32, (need + 7) & ~7u);
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    if(bestEffort)
+    {
+        // headroom only: the new rows must fit beside the old ones, else the
+        // context keeps the lists it has
+        void* probe = nullptr;
+        if(cudaMalloc(&probe, size_t(n) * capN * sizeof(uint32_t)) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return SPH_OK;
+        }
+        cudaFree(probe);
+    }
     if(dc.lists.list)
     {
         auto it = std::find(allocs.begin(), allocs.end(), static_cast<void*>(dc.lists.list));
@@ -938,7 +950,7 @@ int sph_ctx::steps(int32_t nsteps, double dt)
     uint32_t const maxCount = lastStat[sph::kStatMaxCount];
     if(st == SPH_OK && uint64_t(maxCount) * 10 > uint64_t(dc.lists.cap) * 9)
     {
-        int const g = growLists(uint32_t(double(maxCount) * 1.25) + 16);
+        int const g = growLists(uint32_t(double(maxCount) * 1.25) + 16, true);
         if(g)
             return g;
         forceValid = true;
