@@ -218,7 +218,11 @@ int sph_mhd(sph_ctx* ctx);
 /* Replaces: Simulation::runOneStep repeated n_steps times
  * (include/spearhed/control/Simulation.x.cpp:196-310): drift, neighbour search,
  * density, forces, kick.  dt > 0 overrides params.dt for these steps; dt <= 0
- * keeps params.dt (or the CFL dt when SPH_PHYS_CFL is set). */
+ * keeps params.dt (or the CFL dt when SPH_PHYS_CFL is set).  A context whose
+ * species hold no particles steps as a no-op that only advances its clock, as
+ * runOneStep accepts an empty setup (tests/spearhed/unit/SimulationTimestep/
+ * SimulationTimestep.cpp:365-400); sph_density / sph_hydro then do nothing and
+ * sph_reduce reports zero sums. */
 int sph_step(sph_ctx* ctx, int32_t n_steps, double dt);
 
 /* Conserved-quantity reductions of the current state (no reference counterpart;

@@ -63,6 +63,7 @@ namespace
 
     struct HostSpecies
     {
+        bool declared = false; //!< sph_set_species was called, possibly with no particles
         bool set = false;
         uint32_t roles = 0;
         int64_t n = 0;
@@ -185,6 +186,17 @@ struct sph_ctx
     // in any of its steps: the call then regrows the lists and runs again.
     int densityVariant = 0, forceVariant = 0; //!< launch shapes (sph_autotune / sph_set_tuning)
     int64_t replays = 0;                      //!< step calls re-run after a list overflow
+    // A context whose species hold no particles steps as a no-op, as the
+    // reference's runOneStep does on an empty setup; its clock lives here.
+    int64_t emptySteps = 0;
+    double emptyTime = 0.0;
+    bool empty() const
+    {
+        for(auto const& s : sp)
+            if(s.set)
+                return false;
+        return true;
+    }
     bool anyTwoLevel = false;                 //!< some box allocates level-1 cells
     uint32_t lastStat[sph::kStatWords] = {};  //!< status words of the last checkStatus
     SphTuning tuning{};
@@ -1288,6 +1300,7 @@ int sph_set_species(sph_ctx* ctx, int32_t species_id, uint32_t roles, int64_t n,
         return fail(SPH_ERR_INVALID, "sph_set_species: source species need masses");
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     HostSpecies& s = ctx->sp[species_id];
+    s.declared = true;
     if(ctx->allocated && ctx->deviceCurrent && s.set && s.n == n && s.roles == roles)
         return ctx->setSpeciesFast(species_id, v);
     if(ctx->allocated && ctx->mirrorStale)
@@ -1317,6 +1330,8 @@ int sph_density(sph_ctx* ctx)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    if(ctx->empty())
+        return SPH_OK;
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     int st = ctx->ensureDevice();
     if(st || (st = ctx->clearStatus()) || (st = ctx->build(false)) || (st = ctx->densityPass()))
@@ -1346,6 +1361,8 @@ int sph_hydro(sph_ctx* ctx)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    if(ctx->empty())
+        return SPH_OK;
     if(!ctx->densityValid)
         return fail(SPH_ERR_STATE, "sph_hydro needs the density of the current state (call sph_density first)");
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
@@ -1369,6 +1386,12 @@ int sph_step(sph_ctx* ctx, int32_t n_steps, double dt)
 {
     if(!ctx || n_steps < 0 || !std::isfinite(dt))
         return fail(SPH_ERR_INVALID, "sph_step: bad arguments");
+    if(ctx->empty())
+    {
+        ctx->emptySteps += n_steps;
+        ctx->emptyTime += double(n_steps) * (dt > 0.0 ? dt : ctx->p.dt);
+        return SPH_OK;
+    }
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     return ctx->steps(n_steps, dt);
 }
@@ -1378,6 +1401,8 @@ int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* v)
     if(!ctx || !v || species_id < 0 || species_id >= SPH_NUM_SPECIES)
         return fail(SPH_ERR_INVALID, "sph_get_species: bad arguments");
     HostSpecies const& s = ctx->sp[species_id];
+    if(s.declared && s.n == 0)
+        return SPH_OK; // nothing to copy
     if(!s.set)
         return fail(SPH_ERR_STATE, "sph_get_species: species not set");
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
@@ -1451,6 +1476,8 @@ int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts)
     if(!ctx || !counts || species_id < 0 || species_id >= SPH_NUM_SPECIES)
         return fail(SPH_ERR_INVALID, "sph_get_neighbour_counts: bad arguments");
     HostSpecies const& s = ctx->sp[species_id];
+    if(s.declared && s.n == 0)
+        return SPH_OK;
     if(!s.set)
         return fail(SPH_ERR_STATE, "species not set");
     if(!ctx->densityValid)
@@ -1523,6 +1550,14 @@ int sph_reduce(sph_ctx* ctx, SphDiag* out)
 {
     if(!ctx || !out)
         return fail(SPH_ERR_INVALID, "sph_reduce: bad arguments");
+    if(ctx->empty())
+    {
+        *out = SphDiag{};
+        out->steps = ctx->emptySteps;
+        out->time = ctx->emptyTime;
+        out->dt = out->dt_next = ctx->p.dt;
+        return SPH_OK;
+    }
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     std::vector<double> pb;
     sph::StepScalars sc{};
@@ -1554,6 +1589,19 @@ int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
 {
     if(!ctx || !out || nbox < 1)
         return fail(SPH_ERR_INVALID, "sph_ensemble_reduce: bad arguments");
+    if(ctx->empty())
+    {
+        if(size_t(nbox) != std::max<size_t>(1, ctx->boxes.size()))
+            return fail(SPH_ERR_INVALID, "sph_ensemble_reduce: nbox differs from the context's box count");
+        for(int32_t b = 0; b < nbox; ++b)
+        {
+            out[b] = SphDiag{};
+            out[b].steps = ctx->emptySteps;
+            out[b].time = ctx->emptyTime;
+            out[b].dt = out[b].dt_next = ctx->p.dt;
+        }
+        return SPH_OK;
+    }
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     std::vector<double> pb;
     sph::StepScalars sc{};

@@ -110,3 +110,23 @@ def test_tracers_do_not_touch_the_fluid(prec):
     without, _ = _run(*_setup(prec, tracers=False), 3)
     for f in ("pos", "vel", "density", "u", "h"):
         assert np.array_equal(getattr(with_t[abi.SPECIES_DEFAULT], f), getattr(without[abi.SPECIES_DEFAULT], f)), f
+
+
+@pytest.mark.parametrize("sids", [(abi.SPECIES_DEFAULT,), (abi.SPECIES_DEFAULT, abi.SPECIES_BOUNDARY, abi.SPECIES_TRACER)])
+def test_empty_setup_steps(sids):
+    """An empty Default-only or all-species setup steps without error (the
+    reference's runOneStep on an empty setup): the clock advances, the sums
+    are zero and reading the empty species back gives nothing."""
+    import spearhed_b200 as sb
+    params = abi.default_params(dt=2e-3)
+    ctx = sb.Context(params, [abi.make_box((0, 0, 0), (1, 1, 1))])
+    for sid in sids:
+        ctx.set_species(sid, abi.Species(0))
+    ctx.step(3)
+    ctx.density()
+    d = ctx.reduce()
+    assert d["steps"] == 3 and d["time"] == pytest.approx(6e-3)
+    assert d["e_kin"] == d["e_int"] == d["pairs"] == 0 and d["n_targets"] == 0
+    for sid in sids:
+        assert ctx.get_species(sid).n == 0
+    ctx.close()
