@@ -589,8 +589,9 @@ int sph_ctx::allocate()
        || (st = alloc(dc.sortScratch, sph::radixScratchWords(n))))
         return st;
     if((st = alloc(dc.status, sph::kStatWords)) || (st = alloc(dc.scal, 1)) || (st = alloc(dc.diag, sph::kDiagWords))
-       || (st = alloc(dc.work, 1)))
+       || (st = alloc(dc.work, 1)) || (st = alloc(dc.kickDone, 1)))
         return st;
+    SPH_CUDA_TRY(cudaMemsetAsync(dc.kickDone, 0, sizeof(uint32_t), stream));
     if((st = alloc(dc.bs.dt, nbox)) || (st = alloc(dc.bs.time, nbox)) || (st = alloc(dc.bs.lastDt, nbox))
        || (st = alloc(dc.bs.dtBits, nbox)) || (st = alloc(dc.bs.chBits, nbox)) || (st = alloc(dc.bs.hmaxBits, nbox))
        || (st = alloc(dc.bs.hminBits, nbox)) || (st = alloc(dc.activeTotal, 1)))
@@ -901,8 +902,7 @@ int sph_ctx::stepOnce(cudaEvent_t const* ev)
         return st;
     if(ev)
         SPH_CUDA_TRY(cudaEventRecord(ev[3], stream));
-    sph::launchKick(dc, pa, stream);
-    sph::launchFinalize(dc, (p.physics & SPH_PHYS_CFL) != 0, stream);
+    sph::launchKick(dc, pa, (p.physics & SPH_PHYS_CFL) != 0, stream);
     if(ev)
         SPH_CUDA_TRY(cudaEventRecord(ev[4], stream));
     return SPH_OK;

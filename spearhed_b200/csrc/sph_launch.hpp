@@ -215,6 +215,7 @@ namespace sph
         uint32_t* sortScratch;
         uint32_t* status; //!< kStatWords words
         uint32_t* work;   //!< density work queue: next cell to hand out (zeroed before each launch)
+        uint32_t* kickDone; //!< kick blocks finished; the last one finalises the step and resets it
         uint32_t* activeTotal; //!< work items of all boxes (their current cells, both levels)
         int32_t support;       //!< kernel support in units of h
         StepScalars* scal;
@@ -250,7 +251,9 @@ namespace sph
     void launchDriftKeys(DevCtx const& c, bool drift, cudaStream_t s);
     void launchCellRanges(DevCtx const& c, uint32_t const* sortedKeys, cudaStream_t s);
     void launchPermute(DevCtx const& c, uint32_t const* perm, PhysArgs const& pa, int precision, cudaStream_t s);
-    void launchKick(DevCtx const& c, PhysArgs const& pa, cudaStream_t s);
+    //! Kick, adaptive h and the block partials of the conserved sums; the last
+    //! block to finish also finalises the step (sums, clock, next CFL dt).
+    void launchKick(DevCtx const& c, PhysArgs const& pa, bool cfl, cudaStream_t s);
     void launchFinalize(DevCtx const& c, bool cfl, cudaStream_t s);
     void launchUnpermute(uint32_t n, uint32_t const* id, double const* src, double* dst, cudaStream_t s);
     void launchUnpermuteInt(uint32_t n, uint32_t const* id, uint32_t const* src, int32_t* dst, cudaStream_t s);

@@ -192,17 +192,80 @@ namespace sph
         //! Kick (Movable & Thermodynamic): v += dvdt dt, u += dudt dt, and with MHD
         //! B += dBdt dt, psi += dpsidt dt; then FP64 block partial sums of the
         //! conserved quantities of the new state (deterministic: fixed order).
-        __global__ void __launch_bounds__(kThreads) kKick(DevCtx c, PhysArgs pa)
+        //! Step epilogue of one block: the block partials of the conserved sums
+        //! in a fixed order (read through L2: other blocks wrote them), the step
+        //! counters, and every box's clock and next dt.  red holds one row per warp.
+        __device__ void finalizeStep(DevCtx const& c, bool cfl, double (*red)[kDiagWords])
+        {
+            double acc[kDiagWords];
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+                acc[k] = 0.0;
+            for(uint32_t b = threadIdx.x; b < c.nPartialBlocks; b += blockDim.x)
+#pragma unroll
+                for(int k = 0; k < kDiagWords; ++k)
+                {
+                    double const v = __ldcg(&c.partials[size_t(b) * kDiagWords + k]);
+                    acc[k] = (k == 8) ? fmax(acc[k], v) : acc[k] + v;
+                }
+            int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            __syncthreads(); // red is free again
+#pragma unroll
+            for(int k = 0; k < kDiagWords; ++k)
+            {
+                double const r = (k == 8) ? warpMax(acc[k]) : warpSum(acc[k]);
+                if(lane == 0)
+                    red[warp][k] = r;
+            }
+            __syncthreads();
+            if(threadIdx.x == 0)
+            {
+                double tot[kDiagWords];
+#pragma unroll
+                for(int k = 0; k < kDiagWords; ++k)
+                {
+                    tot[k] = 0.0;
+                    for(int w = 0; w < int(blockDim.x / 32); ++w)
+                        tot[k] = (k == 8) ? fmax(tot[k], red[w][k]) : tot[k] + red[w][k];
+                }
+                StepScalars& S = *c.scal;
+                S.steps += 1;
+                S.pairsAccum += double(S.pairs);
+#pragma unroll
+                for(int k = 0; k < 10; ++k)
+                    c.diag[k] = tot[k];
+                c.diag[10] = c.bs.dt[0];
+                c.diag[11] = c.bs.time[0] + c.bs.dt[0];
+            }
+            // every box advances by its own dt; with CFL its next dt is its own minimum
+            for(uint32_t b = threadIdx.x; b < c.nbox; b += blockDim.x)
+            {
+                double const dt = c.bs.dt[b];
+                c.bs.time[b] += dt;
+                c.bs.lastDt[b] = dt;
+                if(cfl)
+                {
+                    double const dtn = __longlong_as_double(static_cast<long long>(c.bs.dtBits[b]));
+                    if(dtn > 0.0 && dtn < 1e300)
+                        c.bs.dt[b] = dtn;
+                }
+            }
+        }
+
+        __global__ void __launch_bounds__(kThreads) kKick(DevCtx c, PhysArgs pa, bool cfl)
         {
             __shared__ double red[kThreads / 32][kDiagWords];
-            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
             double acc[kDiagWords];
 #pragma unroll
             for(int k = 0; k < kDiagWords; ++k)
                 acc[k] = 0.0;
             bool const mhd = pa.physics & SPH_PHYS_MHD;
-            if(p < c.n && isTarget(c.cur.role[p]))
+            // grid-stride: at most a few blocks per SM, so the step's epilogue
+            // sums few block partials
+            for(uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < c.n; p += gridDim.x * blockDim.x)
             {
+                if(!isTarget(c.cur.role[p]))
+                    continue;
                 double const dt = c.bs.dt[c.cur.box[p]];
                 double const m = c.cur.m[p];
                 double v2 = 0.0, B2 = 0.0;
@@ -212,7 +275,7 @@ namespace sph
                     double const va = c.cur.v[a][p] + c.d.dvdt[a][p] * dt;
                     c.cur.v[a][p] = va;
                     v2 += va * va;
-                    acc[3 + a] = m * va;
+                    acc[3 + a] += m * va;
                 }
                 double const u = c.cur.u[p] + c.d.dudt[p] * dt;
                 c.cur.u[p] = u;
@@ -227,25 +290,26 @@ namespace sph
                     }
                     c.cur.psi[p] += c.d.dpsidt[p] * dt;
                 }
-                acc[0] = 0.5 * m * v2;
-                acc[1] = m * u;
+                acc[0] += 0.5 * m * v2;
+                acc[1] += m * u;
                 double const rho = c.cur.rho[p];
                 if(pa.physics & SPH_PHYS_ADAPTIVE_H)
                 {
-                    // h for the next step from this step's density, capped by the cell size
+                    // h for the next step from this step's density, capped by the box's h cap
                     double const hn = pa.hfact * cbrt(m / rho);
                     double const cap = c.boxes[c.cur.box[p]].hcap;
                     c.cur.h[p] = hn < cap ? hn : cap;
                 }
-                acc[2] = (mhd && rho > 0.0) ? 0.5 * m * B2 / (pa.mu0 * rho) : 0.0;
+                if(mhd && rho > 0.0)
+                    acc[2] += 0.5 * m * B2 / (pa.mu0 * rho);
                 if(mhd && B2 > 0.0)
                 {
                     double const e = fabs(c.d.divB[p]) * c.cur.h[p] / sqrt(B2);
-                    acc[6] = e;
-                    acc[7] = 1.0;
-                    acc[8] = e;
+                    acc[6] += e;
+                    acc[7] += 1.0;
+                    acc[8] = fmax(acc[8], e);
                 }
-                acc[9] = 1.0;
+                acc[9] += 1.0;
             }
             int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -263,6 +327,19 @@ namespace sph
                 for(int w = 0; w < kThreads / 32; ++w)
                     r = (k == 8) ? fmax(r, red[w][k]) : r + red[w][k];
                 c.partials[size_t(blockIdx.x) * kDiagWords + k] = r;
+            }
+            // the last block to finish finalises the step (no block waits for another)
+            __shared__ bool last;
+            __threadfence();
+            __syncthreads();
+            if(threadIdx.x == 0)
+                last = atomicAdd(c.kickDone, 1u) == gridDim.x - 1;
+            __syncthreads();
+            if(last)
+            {
+                finalizeStep(c, cfl, red);
+                if(threadIdx.x == 0)
+                    *c.kickDone = 0;
             }
         }
 
@@ -669,7 +746,8 @@ namespace sph
 
     uint32_t partialBlocks(uint32_t n)
     {
-        return (n + kThreads - 1) / kThreads;
+        uint32_t const b = (n + kThreads - 1) / kThreads;
+        return b < 148u * 8u ? b : 148u * 8u;
     }
 
     void launchDriftKeys(DevCtx const& c, bool drift, cudaStream_t s)
@@ -710,13 +788,15 @@ namespace sph
         }
     }
 
-    void launchKick(DevCtx const& c, PhysArgs const& pa, cudaStream_t s)
+    void launchKick(DevCtx const& c, PhysArgs const& pa, bool cfl, cudaStream_t s)
     {
         if(c.n)
         {
-            kKick<<<partialBlocks(c.n), kThreads, 0, s>>>(c, pa);
+            kKick<<<partialBlocks(c.n), kThreads, 0, s>>>(c, pa, cfl);
             countLaunches(1);
         }
+        else
+            launchFinalize(c, cfl, s);
     }
 
     void launchFinalize(DevCtx const& c, bool cfl, cudaStream_t s)
