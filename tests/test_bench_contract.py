@@ -50,3 +50,12 @@ def test_hbm_view_of_a_launch():
     assert v["unit"] == "GB/s" and abs(v["achieved"] - 650.0) < 1e-9 and abs(v["frac"] - 0.1) < 1e-12
     assert bench.hbm_view({"traffic": None, "ms_per_launch": 1.0}, 6500.0) is None
     assert bench.hbm_view({"traffic": 6.5e8, "ms_per_launch": 1.0}, None) is None
+
+
+def test_traffic_only_for_the_profiled_configuration():
+    import argparse
+    a = argparse.Namespace(workload="orszag_tang", nx=512, nz=4)
+    assert bench.profiled_config(a)
+    a.nx = 256
+    assert not bench.profiled_config(a)
+    assert not bench.profiled_config(argparse.Namespace(workload="mhd_rotor", nx=512, nz=4))
