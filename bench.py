@@ -270,7 +270,7 @@ def measured_peak(key):
 
 
 # ------------------------------------------------------- CPU baselines
-def cpu_reference_sample(nx, nz, budget_s=20.0):
+def cpu_reference_sample(nx, nz, limit_s=20.0):
     """The reference's density + hydro functors (compiled from its sources) over
     a sample of target frames of the same workload, driven by its region/frame
     engine restated in oracle/ref_functors.cpp.  Falls back to the oracle port."""
@@ -283,7 +283,7 @@ def cpu_reference_sample(nx, nz, budget_s=20.0):
     if ref is not None and hasattr(ref, "ref_region_bench_f32"):
         box = w.boxes[0]
         side = 4.0 / nx  # regions of 4 x 4 x 4 lattice cells = one 64-slot frame each
-        r = pyoracle.region_bench(s, w.params, list(box.lo), list(box.hi), side, budget_s=budget_s)
+        r = pyoracle.region_bench(s, w.params, list(box.lo), list(box.hi), side, limit_s=limit_s)
         r["cores"] = cores
         return r
     # Oracle port: density + force of the full SPMHD step on a smaller slab of
@@ -300,7 +300,7 @@ def cpu_reference_sample(nx, nz, budget_s=20.0):
         orc.density()
         orc.force()
         reps += 1
-        if time.perf_counter() - t0 > min(budget_s, 10.0):
+        if time.perf_counter() - t0 > min(limit_s, 10.0):
             break
     dt = time.perf_counter() - t0
     return {"value": 3 * pairs * reps / dt, "unit": UNIT, "cores": cores, "kind": "port",
@@ -561,7 +561,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cpu = cpu_reference_sample(args.nx, args.nz, budget_s=max(5.0, 2.0 * args.steps))
+        cpu = cpu_reference_sample(args.nx, args.nz, limit_s=max(5.0, 2.0 * args.steps))
         line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32" if cpu.get("kind") == "reference" else "fp64",

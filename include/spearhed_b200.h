@@ -3,7 +3,7 @@
  * The step this library replaces is spearHED's neighbour-region SPH step as
  * composed by Simulation::runOneStep (include/spearhed/control/Simulation.x.cpp:196-310):
  * drift -> neighbour search -> UpdateDensity -> UpdateHydroForces -> EulerIntegrate.
- * It adds the terms the north-star step needs on top of the reference's
+ * It adds the terms the SPH-MHD step needs on top of the reference's
  * inviscid hydro: artificial viscosity, SPMHD induction and magnetic stress,
  * Dedner divergence cleaning, a CFL time step and FP64 conserved-quantity sums.
  *
@@ -42,7 +42,7 @@ enum
     SPH_ERR_OVERFLOW = 6,      /* a neighbour list exceeded its capacity (retry is automatic) */
     SPH_ERR_STATE = 7,         /* call out of order (e.g. hydro before density)             */
     SPH_ERR_TIMEOUT = 8,       /* a bounded wait on the device gave up                      */
-    SPH_ERR_UNSUPPORTED = 9    /* configuration this build does not implement               */
+    SPH_ERR_UNSUPPORTED = 9    /* configuration the library does not implement              */
 };
 
 /* ---- kernels (SphKernel models, include/spearhed/sph/SphKernel.hpp:45-51) -- */

@@ -203,11 +203,11 @@ def _check(st):
         raise RuntimeError(f"oracle error {st}")
 
 
-def region_bench(species, params, box_lo, box_hi, side, budget_s=20.0, dtype=np.float32):
+def region_bench(species, params, box_lo, box_hi, side, limit_s=20.0, dtype=np.float32):
     """Time the reference's density + hydro functors (compiled from its sources)
     under its region/frame engine on the host cores: regions of edge `side`,
     64-slot frames, cubic spline with the radius 2*h0 of `params`.  Target
-    frames run in order until `budget_s` has passed.  Returns a cpu_baseline dict."""
+    frames run in order until `limit_s` has passed.  Returns a cpu_baseline dict."""
     L = ref()
     T = C.c_float if dtype == np.float32 else C.c_double
     suf = "f32" if dtype == np.float32 else "f64"
@@ -226,7 +226,7 @@ def region_bench(species, params, box_lo, box_hi, side, budget_s=20.0, dtype=np.
     sec = C.c_double(0)
     st = getattr(L, f"ref_region_bench_{suf}")(
         0, n, P(pos), P(mass), P(h), P(rho), P(u), P(vel), P(lo), P(hi), side, 2.0 * params.h0, params.gamma,
-        budget_s, C.byref(pd), C.byref(ph), C.byref(fd), C.byref(ft), C.byref(sec))
+        limit_s, C.byref(pd), C.byref(ph), C.byref(fd), C.byref(ft), C.byref(sec))
     _check(st)
     value = (pd.value + ph.value) / sec.value
     return {"value": value, "unit": "pair-interactions/s", "kind": "reference",

@@ -526,7 +526,7 @@ extern "C"
 
     /** CPU baseline: the reference's density pass then hydro pass (its own
      *  functors) over target frames of a region/frame decomposition of the
-     *  input (regions of edge `side`), processed in order until `budget_s`
+     *  input (regions of edge `side`), processed in order until `limit_s`
      *  seconds have passed or every frame is done; OpenMP over target frames.
      *  Returns accepted non-self pairs of each pass, the frames processed,
      *  and the seconds of the two passes. */
@@ -544,7 +544,7 @@ extern "C"
         T side,
         T radius,
         T gamma,
-        double budget_s,
+        double limit_s,
         int64_t* pairsDensity,
         int64_t* pairsHydro,
         int* framesDone,
@@ -649,7 +649,7 @@ extern "C"
             }
             done = end;
             double const el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            if(el > budget_s)
+            if(el > limit_s)
                 break;
         }
         *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

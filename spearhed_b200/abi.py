@@ -254,7 +254,7 @@ def lib():
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(
             f"spearhed_b200 CUDA library not built: {LIB_PATH} is missing "
-            "(run `python -c 'import __graft_entry__ as g; g.build()'`)")
+            "(run `python -m spearhed_b200.build`)")
     L = C.CDLL(LIB_PATH)
     P = C.POINTER
     ctx_p = C.c_void_p

@@ -35,8 +35,8 @@ Wendland C2 kernel (the benchmark workload's kernel):
     Dedner gradient term and accumulate                          10
                                                                 115
 The SPH pair-interaction metric counts logical pair passes per step: density (1),
-hydro/AV (1) and SPMHD/Dedner (1); this build evaluates the last two in one
-fused force kernel, so one accepted pair of that kernel is two pair interactions.
+hydro/AV (1) and SPMHD/Dedner (1); one fused force kernel evaluates the last
+two, so one accepted pair of that kernel is two pair interactions.
 """
 
 DENSITY_FLOPS = {"cubic": 27, "quintic": 33, "wendland_c2": 27}

@@ -4,7 +4,7 @@ the FP32 path's energy drift against the FP64 path's.
 - Magnetised Kelvin-Helmholtz (two lattices, 2:1 density, jitter, adaptive h,
   pair-max cull) and the MHD rotor (10:1 density disc, rotation, adaptive h):
   two full steps match the oracle; FP64 to round-off, FP32 within the
-  north-star bounds after one step.
+  target error bounds after one step (density 1e-5, accelerations 1e-4).
 - Energy drift: 100 steps of the jittered Orszag-Tang slab, FP32-compensated
   versus FP64 plain; the FP32 run's relative drift of the total energy
   (kinetic + internal + magnetic) stays within 2% of the FP64 run's drift (or
@@ -60,7 +60,7 @@ def test_config_fp64_two_steps_match_oracle(oracle, name):
 
 
 @pytest.mark.parametrize("name", sorted(CONFIGS))
-def test_config_fp32_one_step_within_north_star_bounds(oracle, name):
+def test_config_fp32_one_step_within_target_bounds(oracle, name):
     import spearhed_b200 as sb
     w = CONFIGS[name](abi.PREC_FP32_COMP)
     ctx = sb.context_for(w)

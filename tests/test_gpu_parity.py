@@ -224,7 +224,7 @@ def test_sod_steps_match_oracle(oracle, prec):
     assert dg["e_kin"] + dg["e_int"] == pytest.approx(d.e_kin + d.e_int, rel=1e-6)
 
 
-def test_sod_one_step_fp32_errors_within_north_star_bounds(oracle):
+def test_sod_one_step_fp32_errors_within_target_bounds(oracle):
     """After one step: density rel <= 1e-5, acceleration normwise <= 1e-4 (FP32 vs FP64 oracle)."""
     w = setups.sod_small(precision=abi.PREC_FP32_COMP, scale=0.5)
     ctx = _ctx(w.params, w.boxes, w.species)

@@ -8,7 +8,7 @@ Thermodynamic) with drift-only tracers (Tracer = Movable), three full steps:
 - the walls keep their positions, velocities, densities and energies bit for bit;
 - tracers keep their velocities and move by v t (they are not sources);
 - the fluid matches the oracle run of the same three species (FP64 to
-  round-off, FP32 within the north-star bounds) and stays inside the walls;
+  round-off, FP32 within 1e-4 density and 1e-3 velocity) and stays inside the walls;
 - taking the tracers away changes no bit of the fluid.
 """
 import numpy as np

@@ -1,6 +1,6 @@
 """spearhed_b200.validate on a small Orszag-Tang slab: the FP32 run takes the
 FP64 run's time steps, ends at the same simulated time, and stays within the
-north-star bounds of it (density 1e-5 relative after one step grows slowly;
+target bounds of it (density 1e-5 relative after one step grows slowly;
 here 30 steps are held to 1e-4, and the energy drifts agree)."""
 import pytest
 
