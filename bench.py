@@ -75,7 +75,7 @@ WORKLOADS = {
 }
 
 
-def make_workload(args, precision):
+def make_workload(args, precision, rank=0, world=1):
     from spearhed_b200 import setups
     if args.workload == "orszag_tang":
         return setups.orszag_tang(nx=args.nx, nz=args.nz, precision=precision)
@@ -84,7 +84,8 @@ def make_workload(args, precision):
     if args.workload == "mhd_rotor":
         return setups.mhd_rotor(precision=precision)
     if args.workload == "brio_wu_ensemble":
-        return setups.brio_wu_ensemble(precision=precision)
+        # boxes are independent: each rank builds and steps its own share
+        return setups.brio_wu_ensemble(precision=precision, rank=rank, world=world)
     return setups.sod_small(precision=precision)
 
 
@@ -323,7 +324,9 @@ def run_ours(args, rank, world):
     L.sphx_launch_count.restype = C.c_ulonglong
 
     wl_name, wl_kernel, wl_phys = WORKLOADS[args.workload]
-    w = make_workload(args, abi.PREC_FP32_COMP)
+    # ensembles shard their boxes over the ranks; a single box runs one replica per rank
+    sharded = args.workload == "brio_wu_ensemble" and world > 1
+    w = make_workload(args, abi.PREC_FP32_COMP, rank, world)
     w.params.device = dev
     n = w.n
     ctx = sb.context_for(w)
@@ -412,7 +415,7 @@ def run_ours(args, rank, world):
             # the baseline of the ensemble: the FP64 single-box step looped over boxes
             v64, t64 = fp64_box_loop(args, dev, passes)
         else:
-            w64 = make_workload(args, abi.PREC_FP64)
+            w64 = make_workload(args, abi.PREC_FP64, rank, world)
             w64.params.device = dev
             ctx64 = sb.context_for(w64)
             ctx64.step(args.warmup)
@@ -425,8 +428,8 @@ def run_ours(args, rank, world):
             v64 = passes * (e1["pairs_total"] - e0["pairs_total"]) / (t64[4] * 1e-3)
             ctx64.close()
         # ---- errors of the FP32 step against the FP64 step from the same state
-        wa = make_workload(args, abi.PREC_FP32_COMP)
-        wb = make_workload(args, abi.PREC_FP64)
+        wa = make_workload(args, abi.PREC_FP32_COMP, rank, world)
+        wb = make_workload(args, abi.PREC_FP64, rank, world)
         ca, cb = sb.context_for(wa), sb.context_for(wb)
         ca.step(1)
         cb.step(1)
@@ -438,7 +441,7 @@ def run_ours(args, rank, world):
         ca.close()
         cb.close()
         # ---- end to end through the C ABI with pinned host buffers
-        wi = make_workload(args, abi.PREC_FP32_COMP)
+        wi = make_workload(args, abi.PREC_FP32_COMP, rank, world)
         cols_in = ["pos", "vel", "mass", "h", "density", "u", "B", "psi"]
         cols_out = ["pos", "vel", "density", "u", "B", "psi"]
         # one set of pinned host columns: each step sends them and reads the
@@ -482,14 +485,16 @@ def run_ours(args, rank, world):
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair kernels (compensated), fp64 integration",
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "fp32 pair kernels (compensated), fp64 integration",
             "data": "synthetic Orszag-Tang initial conditions (lattice, analytic v and B)",
             "config": {"workload": wl_name if args.workload != "orszag_tang" or args.nx == 512 else
                        f"orszag_tang_slab_{args.nx}x{args.nx}x{args.nz}", "particles": n, "kernel": wl_kernel,
                        "boxes": len(w.boxes), "neighbours_mean": pairs_step / n,
                        "physics": {"mhd": "hydro+AV+SPMHD+Dedner+CFL", "hydro_av": "hydro+AV+CFL"}[wl_phys]
                        + ("+adaptive_h" if w.params.physics & abi.PHYS_ADAPTIVE_H else ""),
-                       "pair_passes_per_step": passes, "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "pair_passes_per_step": passes,
+                       "parallelism": (f"box_shards{world}" if sharded else f"replicas{world}") if world > 1 else "single",
                        "l2": "working set > L2 (lists ~" + f"{n * 4 * 136 / 1e9:.2f}" + " GB, state ~0.3 GB)",
                        "graph": bool(args.graph),
                        "launch_shapes": {k: tune[k] for k in ("staging_depth", "density_blocks_per_sm",
@@ -498,7 +503,8 @@ def run_ours(args, rank, world):
             "stage_ms_per_step": {"sort_permute": tm[0] / args.steps, "density": dens_ms, "force": force_ms,
                                   "kick_reduce": tm[3] / args.steps},
             "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": t64[4] / args.fp64_steps,
-                           "fp32_speedup": value / v64 if v64 else None,
+                           # per GPU: the FP64 leg runs on rank 0 alone
+                           "fp32_speedup": value / world / v64 if v64 else None,
                            "stage_ms_per_step": {"sort_permute": t64[0] / args.fp64_steps,
                                                  "density": t64[1] / args.fp64_steps,
                                                  "force": t64[2] / args.fp64_steps,

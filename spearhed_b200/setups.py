@@ -316,23 +316,31 @@ def brio_wu_box(n_target=8192, precision=abi.PREC_FP32_COMP, nt=8, box_id=0):
     return params, box, LatticeInit(blocks).generate()
 
 
-def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144):
+def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144, rank=0, world=1):
     """An ensemble of independent Brio-Wu tubes with particle counts drawn
     log-uniform in [n_lo, n_hi] (numpy Philox, key ``seed``).  With the default
     512 boxes this is about 31 M particles.  Every box keeps its own time step.
     The ensemble-wide h_max is 0, so each box sizes its grid from its own
-    largest h (x1.5 under adaptive h, within its periodic extent)."""
+    largest h (x1.5 under adaptive h, within its periodic extent).
+
+    With ``world`` > 1 only the boxes that longest-processing-time assigns to
+    ``rank`` are built (renumbered from 0; their global ids are in
+    ``meta["global_boxes"]``), so each rank generates only its own particles."""
+    from .ensemble import lpt_partition
     rng = np.random.Generator(np.random.Philox(key=seed))
     sizes = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=nbox)).astype(int)
+    mine = np.arange(nbox) if world <= 1 else np.flatnonzero(lpt_partition(sizes, world) == rank)
     boxes, blocks, params = [], [], None
-    for b, nb in enumerate(sizes):
-        p, box, bl = _brio_wu_blocks(int(nb), precision, 8, b)
+    for local, b in enumerate(mine):
+        p, box, bl = _brio_wu_blocks(int(sizes[b]), precision, 8, local)
         boxes.append(box)
         blocks.extend(bl)
         params = p
+    if params is None:  # a rank with no boxes
+        params, _, _ = _brio_wu_blocks(int(n_lo), precision, 8, 0)
     params.h_max = 0.0
     return _workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: LatticeInit(blocks)}, 100,
-                     {"sizes": sizes.tolist(), "seed": seed})
+                     {"sizes": sizes.tolist(), "seed": seed, "global_boxes": mine.tolist()})
 
 
 def kelvin_helmholtz(n_outer=224, n_band=282, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=3):

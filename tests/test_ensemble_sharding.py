@@ -89,3 +89,21 @@ def test_sharded_run_gathers_every_box_over_gloo(tmp_path):
     out = tmp_path / "result.txt"
     mp.start_processes(_worker, args=(2, _free_port(), str(out)), nprocs=2, start_method="spawn")
     assert out.read_text() == "ok"
+
+
+def test_ensemble_setup_builds_only_the_ranks_boxes():
+    """setups.brio_wu_ensemble(rank, world) builds exactly the boxes the LPT
+    partition gives that rank; together the ranks cover the ensemble once."""
+    from spearhed_b200 import setups
+    full = setups.brio_wu_ensemble(nbox=12, n_lo=512, n_hi=2048)
+    seen = []
+    total = 0
+    for r in range(3):
+        w = setups.brio_wu_ensemble(nbox=12, n_lo=512, n_hi=2048, rank=r, world=3)
+        g = w.meta["global_boxes"]
+        seen += g
+        s = w.species[abi.SPECIES_DEFAULT]
+        assert len(w.boxes) == len(g) and set(np.unique(s.box_id)) <= set(range(len(g)))
+        total += s.n
+    assert sorted(seen) == list(range(12))
+    assert total == full.species[abi.SPECIES_DEFAULT].n
