@@ -140,14 +140,15 @@ def test_density_and_pairs_match_oracle(oracle, kernel, prec, cull, vary):
     assert rel <= TOL[prec]["rho"], rel
 
 
+@pytest.mark.parametrize("kernel", [CUBIC, QUINTIC, WENDLAND])
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("h_lo,n", [(0.25, 6000), (0.4, 4000)])
-def test_two_level_grid_pairs_match_oracle(oracle, prec, h_lo, n):
+def test_two_level_grid_pairs_match_oracle(oracle, kernel, prec, h_lo, n):
     """Smoothing lengths spanning 4x and 2.5x under the pair-max cull: the box
     runs two cell levels with 3- or 4-way splits of the level-0 cells (the
     oracle searches one level); the accepted pair sets are the same and the
     densities agree to round-off."""
-    p, boxes, sp = _cloud(CUBIC, prec, n=n, cull=abi.CULL_PAIR_MAX, vary_h=True, h_lo=h_lo)
+    p, boxes, sp = _cloud(kernel, prec, n=n, cull=abi.CULL_PAIR_MAX, vary_h=True, h_lo=h_lo)
     ctx = _ctx(p, boxes, sp)
     ctx.density()
     got = ctx.get_species(abi.SPECIES_DEFAULT)
