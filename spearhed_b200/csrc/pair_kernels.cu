@@ -312,6 +312,72 @@ namespace sph
             return mask;
         }
 
+        //! Acceptance of four consecutive staged candidates for one target (the
+        //! short-chunk path): the same rounded r^2 - R^2 sign test as cullMask32.
+        template<bool PAIRMAX>
+        __device__ __forceinline__ void cull4(
+            float4 const& own,
+            float nRi2,
+            float const* X,
+            float const* Y,
+            float const* Z,
+            float const* H,
+            float R2g,
+            bool acc[4])
+        {
+            float4 const xv = *reinterpret_cast<float4 const*>(X);
+            float4 const yv = *reinterpret_cast<float4 const*>(Y);
+            float4 const zv = *reinterpret_cast<float4 const*>(Z);
+            float4 hv = make_float4(0.f, 0.f, 0.f, 0.f);
+            if constexpr(PAIRMAX)
+                hv = *reinterpret_cast<float4 const*>(H);
+            float2 const ox = make_float2(own.x, own.x);
+            float2 const oy = make_float2(own.y, own.y);
+            float2 const oz = make_float2(own.z, own.z);
+#pragma unroll
+            for(int p = 0; p < 2; ++p)
+            {
+                float2 const dx = __fadd2_rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
+                float2 const dy = __fadd2_rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
+                float2 const dz = __fadd2_rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
+                float2 const r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+                float2 nr = make_float2(-R2g, -R2g);
+                if constexpr(PAIRMAX)
+                {
+                    float const n0 = p ? hv.z : hv.x, n1 = p ? hv.w : hv.y;
+                    nr = make_float2(fminf(nRi2, n0), fminf(nRi2, n1));
+                }
+                float2 const d = __fadd2_rn(r2, nr);
+                acc[2 * p] = d.x < 0.f;
+                acc[2 * p + 1] = d.y < 0.f;
+            }
+        }
+
+        template<bool PAIRMAX>
+        __device__ __forceinline__ void cull4(
+            D4 const& own,
+            double nRi2,
+            double const* X,
+            double const* Y,
+            double const* Z,
+            double const* H,
+            double R2g,
+            bool acc[4])
+        {
+#pragma unroll
+            for(int u = 0; u < 4; ++u)
+            {
+                double const dx = __dadd_rn(own.x, X[u]);
+                double const dy = __dadd_rn(own.y, Y[u]);
+                double const dz = __dadd_rn(own.z, Z[u]);
+                double const r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                double nR2 = -R2g;
+                if constexpr(PAIRMAX)
+                    nR2 = fmin(nRi2, H[u]);
+                acc[u] = __dadd_rn(r2, nR2) < 0.0;
+            }
+        }
+
         //! Per-lane state of one chunk of up to 32 targets of a cell.
         template<typename V4, typename T>
         struct TargetChunk
@@ -416,43 +482,51 @@ namespace sph
                 }
                 return;
             }
-            // Short chunk: S lanes per target test interleaved candidates
-            // q = q0 + u*S + sub; ballots keep the candidate order.
-            constexpr int U = 4;
+            // Short chunk: S lanes per target; sub-lane s tests the four consecutive
+            // candidates q0 + 4s .. q0 + 4s + 3 (vector loads, paired arithmetic),
+            // and an exclusive scan of the accepted counts over the target's S
+            // lanes places the entries in candidate order.  The window is
+            // far-padded to a multiple of 32, so a block of four that starts
+            // before m is staged whole.
             uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
             int const S = ch.S;
-            for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(U * S))
+            for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(4 * S))
             {
-                bool accU[U];
-                uint32_t entU[U];
-#pragma unroll
-                for(int u = 0; u < U; ++u)
+                uint32_t const qb = q0 + uint32_t(4 * ch.sub);
+                bool acc[4] = {false, false, false, false};
+                uint4 ent = make_uint4(0, 0, 0, 0);
+                if(ch.act && qb < m)
                 {
-                    uint32_t const q = q0 + uint32_t(u * S + ch.sub);
-                    bool const ok = ch.act && q < m;
-                    uint32_t const qq = ok ? q : 0u;
-                    T const dx = addRn(ch.own.x, sNX[qq]);
-                    T const dy = addRn(ch.own.y, sNY[qq]);
-                    T const dz = addRn(ch.own.z, sNZ[qq]);
-                    T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
-                    T R2 = R2g;
-                    if constexpr(PAIRMAX)
-                        R2 = -(ch.nR2 < sH[qq] ? ch.nR2 : sH[qq]);
-                    entU[u] = sEnt[qq];
-                    accU[u] = ok && r2 < R2 && entU[u] != selfEnt;
+                    cull4<PAIRMAX>(ch.own, ch.nR2, sNX + qb, sNY + qb, sNZ + qb, sH + qb, R2g, acc);
+                    ent = *reinterpret_cast<uint4 const*>(sEnt + qb);
+                    acc[0] = acc[0] && ent.x != selfEnt;
+                    acc[1] = acc[1] && ent.y != selfEnt;
+                    acc[2] = acc[2] && ent.z != selfEnt;
+                    acc[3] = acc[3] && ent.w != selfEnt;
                 }
-#pragma unroll
-                for(int u = 0; u < U; ++u)
+                uint32_t const cnt = uint32_t(acc[0]) + uint32_t(acc[1]) + uint32_t(acc[2]) + uint32_t(acc[3]);
+                uint32_t incl = cnt;
+                for(int d = 1; d < S; d <<= 1)
                 {
-                    uint32_t const bits = __ballot_sync(0xffffffffu, accU[u]) & ch.groupMask;
-                    if(accU[u])
-                    {
-                        uint32_t const k = ch.nl + __popc((bits >> ch.groupBase) & ch.subBelow);
-                        if(!countOnly && k < cap)
-                            row[k] = entU[u];
-                    }
-                    ch.nl += __popc(bits);
+                    uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d, S);
+                    if(ch.sub >= d)
+                        incl += o;
                 }
+                uint32_t const total = __shfl_sync(0xffffffffu, incl, S - 1, S);
+                if(!countOnly)
+                {
+                    uint32_t k = ch.nl + incl - cnt;
+                    uint32_t const e[4] = {ent.x, ent.y, ent.z, ent.w};
+#pragma unroll
+                    for(int u = 0; u < 4; ++u)
+                        if(acc[u])
+                        {
+                            if(k < cap)
+                                row[k] = e[u];
+                            ++k;
+                        }
+                }
+                ch.nl += total;
             }
         }
 
