@@ -174,6 +174,7 @@ struct sph_ctx
     std::vector<double*> staging;
     bool useGraph = false;
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    unsigned graphKernels[2] = {0, 0}; //!< kernels in each captured two-step graph
     int parity = 0;
     std::vector<cudaEvent_t> events;
     cudaEvent_t eCall = nullptr; //!< start of a step call (before its snapshot)
@@ -1090,10 +1091,15 @@ int sph_ctx::runSteps(int32_t nsteps)
             if(!g)
             {
                 cudaGraph_t raw = nullptr;
+                unsigned long long const before = sph::launchesSoFar();
                 SPH_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
                 int const s1 = stepOnce(nullptr);
                 int const s2 = s1 ? s1 : stepOnce(nullptr);
                 cudaError_t const ce = cudaStreamEndCapture(stream, &raw);
+                // the captured launches ran nothing yet: they count when the graph runs
+                unsigned long long const recorded = sph::launchesSoFar() - before;
+                sph::uncountLaunches(recorded);
+                graphKernels[parity] = unsigned(recorded);
                 if(s2)
                     return s2;
                 SPH_CUDA_TRY(ce);
@@ -1102,6 +1108,7 @@ int sph_ctx::runSteps(int32_t nsteps)
                 SPH_CUDA_TRY(ie);
             }
             SPH_CUDA_TRY(cudaGraphLaunch(g, stream));
+            sph::countLaunches(graphKernels[parity]);
             done += 2;
         }
     }

@@ -46,6 +46,16 @@ namespace sph
     {
         g_launches.fetch_add(k, std::memory_order_relaxed);
     }
+
+    unsigned long long launchesSoFar()
+    {
+        return g_launches.load(std::memory_order_relaxed);
+    }
+
+    void uncountLaunches(unsigned long long k)
+    {
+        g_launches.fetch_sub(k, std::memory_order_relaxed);
+    }
 } // namespace sph
 
 extern "C" {

@@ -230,6 +230,10 @@ namespace sph
 
     //! Adds k to the library's kernel-launch counter (measure.cu).
     void countLaunches(unsigned k);
+    //! The counter's value; and taking back launches that were only recorded
+    //! into a CUDA graph (a graph's kernels count each time it is launched).
+    unsigned long long launchesSoFar();
+    void uncountLaunches(unsigned long long k);
 
     // ---- sort.cu
     size_t scanScratchWords(uint32_t m);
