@@ -252,6 +252,11 @@ int sph_set_clock(sph_ctx* ctx, int32_t nbox, const double* time, const double* 
  * replay it (on = 1) or launch the kernels one by one (on = 0, the default). */
 int sph_use_graph(sph_ctx* ctx, int32_t on);
 
+/* With graph replay on: capture the graph the next sph_step will replay by
+ * running two steps from a snapshot and restoring it, so the capture costs no
+ * simulated time and no later step call pays for it (no reference counterpart). */
+int sph_prepare_graph(sph_ctx* ctx);
+
 /* Launch shapes of the two pair kernels (no reference counterpart; the
  * reference's frame size and threads per frame are compile-time constants,
  * spmacc/Frame.hpp:49-132).  density: staging depth (candidates per shared-memory

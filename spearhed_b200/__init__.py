@@ -111,6 +111,11 @@ class Context:
     def use_graph(self, on: bool = True):
         abi.check(self._L.sph_use_graph(self._p, int(bool(on))))
 
+    def prepare_graph(self):
+        """Capture the graph the next step call replays, from a snapshot that is
+        then restored (no simulated time passes)."""
+        abi.check(self._L.sph_prepare_graph(self._p))
+
     def init_lattice(self, species_id: int, init, roles: int | None = None) -> int:
         """Generates a species on the device from a setups.LatticeInit (lattice
         blocks + profile) and sets it; returns its particle count."""

@@ -274,6 +274,7 @@ def lib():
         "sph_get_neighbour_counts": (C.c_int, [ctx_p, C.c_int32, P(C.c_int32)]),
         "sph_get_timings": (C.c_int, [ctx_p, C.c_int32, P(C.c_double)]),
         "sph_use_graph": (C.c_int, [ctx_p, C.c_int32]),
+        "sph_prepare_graph": (C.c_int, [ctx_p]),
         "sph_get_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_set_clock": (C.c_int, [ctx_p, C.c_int32, P(C.c_double), P(C.c_double)]),
         "sph_autotune": (C.c_int, [ctx_p, C.c_int32, P(SphTuning)]),

@@ -175,6 +175,12 @@ struct sph_ctx
     bool useGraph = false;
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
     unsigned graphKernels[2] = {0, 0}; //!< kernels in each captured two-step graph
+    // Each captured graph records the stage-boundary events of its two steps; before
+    // every replay its event-record nodes are pointed at that replay's own events,
+    // so graph steps are timed per stage like eager ones.
+    cudaGraph_t graphRaw[2] = {nullptr, nullptr};
+    cudaEvent_t graphEv[2][10] = {};
+    cudaGraphNode_t graphEvNode[2][10] = {};
     int parity = 0;
     std::vector<cudaEvent_t> events;
     cudaEvent_t eCall = nullptr; //!< start of a step call (before its snapshot)
@@ -211,6 +217,10 @@ struct sph_ctx
         release();
         for(cudaEvent_t e : events)
             cudaEventDestroy(e);
+        for(auto& row : graphEv)
+            for(cudaEvent_t e : row)
+                if(e)
+                    cudaEventDestroy(e);
         if(eCall)
             cudaEventDestroy(eCall);
         if(eCopy)
@@ -242,6 +252,12 @@ struct sph_ctx
             {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
+            }
+        for(auto& r : graphRaw)
+            if(r)
+            {
+                cudaGraphDestroy(r);
+                r = nullptr;
             }
     }
 
@@ -390,10 +406,11 @@ struct sph_ctx
     int snapshot(bool restore);
     int runSteps(int32_t nsteps);
     int autotune(int32_t stepsPerTrial);
+    int prepareGraph();
     void describeTuning();
     int densityPass();
     int forcePass();
-    int stepOnce(cudaEvent_t const* ev);
+    int stepOnce(cudaEvent_t const* ev, bool capture = false);
     int steps(int32_t nsteps, double dt);
     int setSpeciesFast(int32_t id, SphSoAView const* v);
 };
@@ -886,26 +903,32 @@ int sph_ctx::checkStatus(char const* where)
 }
 
 //! One runOneStep; ev (5 events or null) brackets build / density / force / kick.
-int sph_ctx::stepOnce(cudaEvent_t const* ev)
+//! Under stream capture the events are recorded as external events, so they
+//! become event-record nodes of the graph (retargeted before each replay).
+int sph_ctx::stepOnce(cudaEvent_t const* ev, bool capture)
 {
+    auto recordStage = [&](cudaEvent_t e, bool cap)
+    {
+        return cap ? cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal) : cudaEventRecord(e, stream);
+    };
     int st;
     if(ev)
-        SPH_CUDA_TRY(cudaEventRecord(ev[0], stream));
+        SPH_CUDA_TRY(recordStage(ev[0], capture));
     if((st = build(true)))
         return st;
     if(ev)
-        SPH_CUDA_TRY(cudaEventRecord(ev[1], stream));
+        SPH_CUDA_TRY(recordStage(ev[1], capture));
     if((st = densityPass()))
         return st;
     if(ev)
-        SPH_CUDA_TRY(cudaEventRecord(ev[2], stream));
+        SPH_CUDA_TRY(recordStage(ev[2], capture));
     if((st = forcePass()))
         return st;
     if(ev)
-        SPH_CUDA_TRY(cudaEventRecord(ev[3], stream));
+        SPH_CUDA_TRY(recordStage(ev[3], capture));
     sph::launchKick(dc, pa, (p.physics & SPH_PHYS_CFL) != 0, stream);
     if(ev)
-        SPH_CUDA_TRY(cudaEventRecord(ev[4], stream));
+        SPH_CUDA_TRY(recordStage(ev[4], capture));
     return SPH_OK;
 }
 
@@ -968,6 +991,34 @@ int sph_ctx::steps(int32_t nsteps, double dt)
             return g;
         forceValid = true;
     }
+    return st;
+}
+
+//! Captures the two-step graph of the current buffer parity by running two
+//! steps from a snapshot, then puts the state (particles, clocks, counters)
+//! back: the next sph_step replays the graph from the state it would have
+//! started from anyway.  List overflows during the capture steps regrow the
+//! lists as in a step call.
+int sph_ctx::prepareGraph()
+{
+    int st = ensureDevice();
+    if(st || (st = snapshot(false)))
+        return st;
+    for(int attempt = 0; attempt < 8; ++attempt)
+    {
+        st = runSteps(2);
+        int const rs = snapshot(true);
+        if(rs)
+            return rs;
+        if(st != SPH_ERR_OVERFLOW)
+            break;
+        uint32_t stat[sph::kStatWords];
+        SPH_CUDA_TRY(cudaMemcpy(stat, dc.status, sizeof(stat), cudaMemcpyDeviceToHost));
+        if((st = growLists(uint32_t(double(stat[sph::kStatOverflow]) * 1.25) + 16)))
+            return st;
+    }
+    densityValid = false;
+    forceValid = false;
     return st;
 }
 
@@ -1090,44 +1141,86 @@ int sph_ctx::runSteps(int32_t nsteps)
             cudaGraphExec_t& g = graphs[parity];
             if(!g)
             {
+                cudaEvent_t* const gev = graphEv[parity];
+                for(int k = 0; k < 10; ++k)
+                    if(!gev[k])
+                        SPH_CUDA_TRY(cudaEventCreate(&gev[k]));
                 cudaGraph_t raw = nullptr;
                 unsigned long long const before = sph::launchesSoFar();
                 SPH_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-                int const s1 = stepOnce(nullptr);
-                int const s2 = s1 ? s1 : stepOnce(nullptr);
+                int const s1 = stepOnce(gev, true);
+                int const s2 = s1 ? s1 : stepOnce(gev + 5, true);
                 cudaError_t const ce = cudaStreamEndCapture(stream, &raw);
                 // the captured launches ran nothing yet: they count when the graph runs
                 unsigned long long const recorded = sph::launchesSoFar() - before;
                 sph::uncountLaunches(recorded);
                 graphKernels[parity] = unsigned(recorded);
                 if(s2)
+                {
+                    if(raw)
+                        cudaGraphDestroy(raw);
                     return s2;
+                }
                 SPH_CUDA_TRY(ce);
+                // find the event-record node of each captured stage event
+                size_t nn = 0;
+                SPH_CUDA_TRY(cudaGraphGetNodes(raw, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                SPH_CUDA_TRY(cudaGraphGetNodes(raw, nodes.data(), &nn));
+                int found = 0;
+                for(cudaGraphNode_t nd : nodes)
+                {
+                    cudaGraphNodeType ty;
+                    SPH_CUDA_TRY(cudaGraphNodeGetType(nd, &ty));
+                    if(ty != cudaGraphNodeTypeEventRecord)
+                        continue;
+                    cudaEvent_t ev = nullptr;
+                    SPH_CUDA_TRY(cudaGraphEventRecordNodeGetEvent(nd, &ev));
+                    for(int k = 0; k < 10; ++k)
+                        if(ev == gev[k])
+                        {
+                            graphEvNode[parity][k] = nd;
+                            ++found;
+                        }
+                }
                 cudaError_t const ie = cudaGraphInstantiate(&g, raw, 0);
-                cudaGraphDestroy(raw);
-                SPH_CUDA_TRY(ie);
+                if(ie != cudaSuccess || found != 10)
+                {
+                    cudaGraphDestroy(raw);
+                    if(ie == cudaSuccess)
+                    {
+                        cudaGraphExecDestroy(g);
+                        g = nullptr;
+                    }
+                    SPH_CUDA_TRY(ie);
+                    return fail(SPH_ERR_CUDA, "sph_step: captured graph lacks its stage events");
+                }
+                graphRaw[parity] = raw;
             }
+            // this replay's stage events
+            for(int i = 0; i < 2; ++i)
+                for(int k = 0; k < 5; ++k)
+                    SPH_CUDA_TRY(cudaGraphExecEventRecordNodeSetEvent(
+                        g, graphEvNode[parity][i * 5 + k], events[2 + size_t(done + i) * 5 + k]));
             SPH_CUDA_TRY(cudaGraphLaunch(g, stream));
             sph::countLaunches(graphKernels[parity]);
             done += 2;
         }
     }
-    int32_t const eager0 = done;
     for(; done < nsteps; ++done)
-        if((st = stepOnce(graph ? nullptr : &events[2 + size_t(done) * 5])))
+        if((st = stepOnce(&events[2 + size_t(done) * 5])))
             return st;
     SPH_CUDA_TRY(cudaEventRecord(eEnd, stream));
     st = checkStatus("sph_step");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, eBeg, eEnd);
     timings[4] = ms;
-    if(!graph)
-        for(int32_t s = eager0; s < nsteps; ++s)
-            for(int k = 0; k < 4; ++k)
-            {
-                cudaEventElapsedTime(&ms, events[2 + size_t(s) * 5 + k], events[2 + size_t(s) * 5 + k + 1]);
-                timings[k] += ms;
-            }
+    for(int32_t s = 0; s < nsteps; ++s)
+        for(int k = 0; k < 4; ++k)
+        {
+            cudaEventElapsedTime(&ms, events[2 + size_t(s) * 5 + k], events[2 + size_t(s) * 5 + k + 1]);
+            timings[k] += ms;
+        }
     return st;
 }
 
@@ -1678,6 +1771,16 @@ int sph_use_graph(sph_ctx* ctx, int32_t on)
         return fail(SPH_ERR_INVALID, "null context");
     ctx->useGraph = on != 0;
     return SPH_OK;
+}
+
+int sph_prepare_graph(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    if(!ctx->useGraph || ctx->empty())
+        return SPH_OK;
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    return ctx->prepareGraph();
 }
 
 

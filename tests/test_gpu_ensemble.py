@@ -127,3 +127,32 @@ def test_list_overflow_in_a_step_call_replays_from_its_start(prec):
     # the call ran again once its lists had grown; the reference run never did
     assert dg["replays"] >= 1 and dref[0]["replays"] == 0
     assert dg["list_capacity"] > 32 and dref[0]["list_capacity"] == 256
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32_COMP])
+def test_prepared_graph_leaves_the_state_and_replays_like_eager(prec):
+    """sph_prepare_graph captures the next graph from a snapshot it restores:
+    the clock and step count do not move, and the following steps (replayed)
+    give the bits of eager steps from the same start."""
+    import spearhed_b200 as sb
+    w = setups.orszag_tang(nx=32, nz=4, precision=prec, jitter=0.1)
+    eager = sb.context_for(w)
+    eager.step(2)
+    eager.step(4)
+    ref = eager.get_species(abi.SPECIES_DEFAULT)
+    dref = eager.reduce()
+    eager.close()
+    g = sb.context_for(w)
+    g.use_graph(True)
+    g.step(2)
+    d0 = g.reduce()
+    g.prepare_graph()
+    d1 = g.reduce()
+    assert d1["steps"] == d0["steps"] == 2 and d1["time"] == d0["time"]
+    g.step(4)
+    got = g.get_species(abi.SPECIES_DEFAULT)
+    d = g.reduce()
+    g.close()
+    assert d["steps"] == dref["steps"] == 6 and d["time"] == dref["time"]
+    for f in FIELDS:
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
