@@ -203,7 +203,7 @@ namespace sph
 
         //! Lanes per target for a chunk of nt targets (power of two, nt * S <= 32):
         //! a full chunk gives every lane its own target; a short chunk spreads each
-        //! target over S lanes that sweep interleaved candidates.
+        //! target over S lanes that take consecutive blocks of four candidates.
         __device__ __forceinline__ int subLanes(uint32_t nt)
         {
             return nt > 16 ? 1 : (nt > 8 ? 2 : (nt > 4 ? 4 : (nt > 2 ? 8 : (nt > 1 ? 16 : 32))));

@@ -343,57 +343,11 @@ namespace sph
             }
         }
 
-        //! Sums the block partials in a fixed order and advances time (and the
-        //! CFL dt when enabled).
+        //! The step epilogue on its own (a step with no particle to kick).
         __global__ void __launch_bounds__(kThreads) kFinalize(DevCtx c, bool cfl)
         {
-            __shared__ double red[kThreads][kDiagWords];
-            double acc[kDiagWords];
-#pragma unroll
-            for(int k = 0; k < kDiagWords; ++k)
-                acc[k] = 0.0;
-            for(uint32_t b = threadIdx.x; b < c.nPartialBlocks; b += kThreads)
-#pragma unroll
-                for(int k = 0; k < kDiagWords; ++k)
-                    acc[k] = (k == 8) ? fmax(acc[k], c.partials[size_t(b) * kDiagWords + k])
-                                      : acc[k] + c.partials[size_t(b) * kDiagWords + k];
-#pragma unroll
-            for(int k = 0; k < kDiagWords; ++k)
-                red[threadIdx.x][k] = acc[k];
-            __syncthreads();
-            for(int s = kThreads / 2; s > 0; s >>= 1)
-            {
-                if(int(threadIdx.x) < s)
-#pragma unroll
-                    for(int k = 0; k < kDiagWords; ++k)
-                        red[threadIdx.x][k] = (k == 8) ? fmax(red[threadIdx.x][k], red[threadIdx.x + s][k])
-                                                       : red[threadIdx.x][k] + red[threadIdx.x + s][k];
-                __syncthreads();
-            }
-            if(threadIdx.x == 0)
-            {
-                StepScalars& S = *c.scal;
-                S.steps += 1;
-                S.pairsAccum += double(S.pairs);
-#pragma unroll
-                for(int k = 0; k < 10; ++k)
-                    c.diag[k] = red[0][k];
-                c.diag[10] = c.bs.dt[0];
-                c.diag[11] = c.bs.time[0] + c.bs.dt[0];
-            }
-            // every box advances by its own dt; with CFL its next dt is its own minimum
-            for(uint32_t b = threadIdx.x; b < c.nbox; b += kThreads)
-            {
-                double const dt = c.bs.dt[b];
-                c.bs.time[b] += dt;
-                c.bs.lastDt[b] = dt;
-                if(cfl)
-                {
-                    double const dtn = __longlong_as_double(static_cast<long long>(c.bs.dtBits[b]));
-                    if(dtn > 0.0 && dtn < 1e300)
-                        c.bs.dt[b] = dtn;
-                }
-            }
+            __shared__ double red[kThreads / 32][kDiagWords];
+            finalizeStep(c, cfl, red);
         }
 
         __global__ void kUnpermute(uint32_t n, uint32_t const* __restrict__ id, double const* __restrict__ src, double* __restrict__ dst)
