@@ -201,6 +201,29 @@ namespace sph
             return v;
         }
 
+        template<typename T>
+        __device__ __forceinline__ T warpMinT(T v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+            {
+                T const w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = w < v ? w : v;
+            }
+            return v;
+        }
+        template<typename T>
+        __device__ __forceinline__ T warpMaxT(T v)
+        {
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+            {
+                T const w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = w > v ? w : v;
+            }
+            return v;
+        }
+
         //! Lanes per target for a chunk of nt targets (power of two, nt * S <= 32):
         //! a full chunk gives every lane its own target; a short chunk spreads each
         //! target over S lanes that take consecutive blocks of four candidates.
@@ -438,7 +461,6 @@ namespace sph
             T const* sH,
             uint32_t const* sEnt,
             uint32_t m,
-            uint32_t qSelf,
             T supT,
             T R2g,
             uint32_t* list,
@@ -446,21 +468,18 @@ namespace sph
             bool countOnly)
         {
             uint32_t* const row = list + size_t(ch.t) * cap;
+            // the target itself: its own entry (centre slot), accepted once at r = 0
+            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
             if(ch.S == 1)
             {
                 // Full chunk: every lane its own target; all lanes read the same
                 // 32 candidates (shared-memory broadcast) and build a 32-bit
-                // acceptance mask, then append the accepted entries.  The target
-                // itself is recognised by its staged index (qSelf, or ~0 when it
-                // is not in this window).
-                uint32_t const mySelf = ch.act ? qSelf : 0xffffffffu;
+                // acceptance mask, then append the accepted entries other than the
+                // target's own (a count-only pass counts it; the caller takes it off).
                 for(uint32_t q0 = 0; q0 < m; q0 += 32)
                 {
                     uint32_t mask
                         = cullMask32<PAIRMAX>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
-                    uint32_t const rel = mySelf - q0;
-                    if(rel < 32u)
-                        mask &= ~(0x80000000u >> rel);
                     if(!ch.act)
                         mask = 0;
                     if(countOnly)
@@ -474,7 +493,10 @@ namespace sph
                     {
                         uint32_t const u = uint32_t(__clz(mask));
                         mask &= 0x7fffffffu >> u;
-                        ch.buf = make_uint4(ch.buf.y, ch.buf.z, ch.buf.w, sEnt[q0 + u]);
+                        uint32_t const e = sEnt[q0 + u];
+                        if(e == selfEnt)
+                            continue;
+                        ch.buf = make_uint4(ch.buf.y, ch.buf.z, ch.buf.w, e);
                         ++ch.nl;
                         if((ch.nl & 3u) == 0 && ch.nl <= cap)
                             *reinterpret_cast<uint4*>(row + (ch.nl - 4)) = ch.buf;
@@ -488,7 +510,6 @@ namespace sph
             // lanes places the entries in candidate order.  The window is
             // far-padded to a multiple of 32, so a block of four that starts
             // before m is staged whole.
-            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
             int const S = ch.S;
             for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(4 * S))
             {
@@ -755,7 +776,6 @@ namespace sph
                 // of those 27 cells.  Each carries its source range and the level-0
                 // stencil slot of its image.
                 int const nDesc = 27 + (B.levels == 2 ? 27 : 0);
-                int const selfDesc = lt ? 27 + kCentreSlot : kCentreSlot;
                 auto describe = [&](int d, uint32_t& sBeg, uint32_t& sCnt, uint32_t& slot, T sh[3])
                 {
                     sBeg = 0;
@@ -865,6 +885,34 @@ namespace sph
                     initChunk(A, rec, tc, tEnd, lane, supT);
                     bool const twoChunks = tc + 32 < tEnd;
                     initChunk(Bc, rec, tc + 32, tEnd, lane, supT);
+                    uint32_t const nTargets = min(32u, tEnd - tc) + (twoChunks ? min(32u, tEnd - tc - 32) : 0u);
+                    // Bounding box of the two chunks' targets and their largest cull
+                    // radius: staging keeps only candidates within that radius of the
+                    // box.  For a target x_i in [lo, hi] and a staged -x_j, rounding
+                    // is monotone, so |x_i - x_j| (rounded) >= max(lo - x_j, x_j - hi,
+                    // 0) (rounded) on each axis; with the radius widened by 2^-10 the
+                    // box test passes every candidate the exact cull accepts.
+                    T bLo[3], bHi[3];
+                    {
+                        T const inf = T(kFar);
+                        T const ax[3] = {A.own.x, A.own.y, A.own.z}, bx[3] = {Bc.own.x, Bc.own.y, Bc.own.z};
+#pragma unroll
+                        for(int a = 0; a < 3; ++a)
+                        {
+                            T const l0 = A.act ? ax[a] : inf, l1 = Bc.act ? bx[a] : inf;
+                            T const h0 = A.act ? ax[a] : -inf, h1 = Bc.act ? bx[a] : -inf;
+                            bLo[a] = warpMinT<T>(l0 < l1 ? l0 : l1);
+                            bHi[a] = warpMaxT<T>(h0 > h1 ? h0 : h1);
+                        }
+                    }
+                    T const widen = T(1) + T(1.0 / 1024.0);
+                    // PAIRMAX: the pair radius is max(R_i, R_j); nRt = -(max_i R_i)^2
+                    T nRt = -R2g;
+                    if constexpr(PAIRMAX)
+                    {
+                        T const nA = A.act ? A.nR2 : T(0), nB = Bc.act ? Bc.nR2 : T(0);
+                        nRt = warpMinT<T>(nA < nB ? nA : nB);
+                    }
                     for(int page = 0; page * 32 < nDesc; ++page)
                     {
                     uint32_t sBeg = sBeg0, sCnt = sCnt0, slotD = slot0, pre = pre0, total = total0;
@@ -874,7 +922,6 @@ namespace sph
                         describe(page * 32 + lane, sBeg, sCnt, slotD, sh);
                         scan(sCnt, pre, total);
                     }
-                    int const selfLane = selfDesc - page * 32;
                     // entry of staged position q: eBase of q's descriptor + (q << 5)
                     // (j = sBeg + q - pre, packed as (j << 5) | slot)
                     uint32_t const eBase = ((sBeg - pre) << 5) | slotD;
@@ -882,12 +929,15 @@ namespace sph
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
                         __syncwarp();
-                        // Flat staging: lane l fills window positions l, l + 32, ...; the
+                        // Flat staging: lane l reads window positions l, l + 32, ...; the
                         // descriptor of position q is the last one whose prefix is <= q
                         // (a shuffle binary search over the page's prefixes; empty
                         // descriptors share the next one's prefix and are passed over).
-                        // kStageBatch positions' records are in flight at once.
+                        // kStageBatch positions' records are in flight at once.  The
+                        // candidates that pass the box test are staged in order at
+                        // 0 .. m-1.
                         constexpr int KB = PairCfg<T>::kStageBatch;
+                        uint32_t mW = 0; // staged so far (warp-uniform)
 #pragma unroll 1
                         for(uint32_t k0 = 0; cb + 32u * k0 < ce; k0 += KB)
                         {
@@ -919,25 +969,39 @@ namespace sph
 #pragma unroll
                             for(int k = 0; k < KB; ++k)
                             {
-                                uint32_t const w = uint32_t(lane) + 32u * (k0 + uint32_t(k));
+                                bool const in = cb + uint32_t(lane) + 32u * (k0 + uint32_t(k)) < ce;
                                 T const sx = __shfl_sync(0xffffffffu, sh[0], dsc[k]);
                                 T const sy = __shfl_sync(0xffffffffu, sh[1], dsc[k]);
                                 T const sz = __shfl_sync(0xffffffffu, sh[2], dsc[k]);
-                                if(cb + w < ce)
+                                T const nx = in ? -addRn(pj[k].x, sx) : T(kFar);
+                                T const ny = in ? -addRn(pj[k].y, sy) : T(kFar);
+                                T const nz = in ? -addRn(pj[k].z, sz) : T(kFar);
+                                T nRj = T(0);
+                                if constexpr(PAIRMAX)
                                 {
-                                    sNX[w] = -addRn(pj[k].x, sx);
-                                    sNY[w] = -addRn(pj[k].y, sy);
-                                    sNZ[w] = -addRn(pj[k].z, sz);
+                                    T const Rj = mulRn(supT, in ? hj[k] : T(0));
+                                    nRj = -mulRn(Rj, Rj);
+                                }
+                                T const dx = fmax(fmax(addRn(bLo[0], nx), -addRn(bHi[0], nx)), T(0));
+                                T const dy = fmax(fmax(addRn(bLo[1], ny), -addRn(bHi[1], ny)), T(0));
+                                T const dz = fmax(fmax(addRn(bLo[2], nz), -addRn(bHi[2], nz)), T(0));
+                                T const nR = (nRj < nRt ? nRj : nRt) * widen;
+                                bool const pass = in && dx * dx + dy * dy + dz * dz + nR < T(0);
+                                uint32_t const passMask = __ballot_sync(0xffffffffu, pass);
+                                if(pass)
+                                {
+                                    uint32_t const w = mW + uint32_t(__popc(passMask & ((1u << lane) - 1u)));
+                                    sNX[w] = nx;
+                                    sNY[w] = ny;
+                                    sNZ[w] = nz;
                                     sEnt[w] = ent[k];
                                     if constexpr(PAIRMAX)
-                                    {
-                                        T const Rj = mulRn(supT, hj[k]);
-                                        sH[w] = -mulRn(Rj, Rj);
-                                    }
+                                        sH[w] = nRj;
                                 }
+                                mW += uint32_t(__popc(passMask));
                             }
                         }
-                        uint32_t const m = ce - cb;
+                        uint32_t const m = mW;
                         // far candidates up to the next multiple of 32
                         for(uint32_t q = m + uint32_t(lane); q < ((m + 31u) & ~31u); q += 32)
                         {
@@ -948,24 +1012,21 @@ namespace sph
                                 sH[q] = T(0);
                         }
                         __syncwarp();
-                        // staged index of a target = its own cell's window offset + its rank
-                        // in the cell, on the page that holds its own cell
-                        bool const selfPage = selfLane >= 0 && selfLane < 32;
-                        uint32_t const cPre = __shfl_sync(0xffffffffu, pre, selfPage ? selfLane : 0);
-                        uint32_t const cBeg = __shfl_sync(0xffffffffu, sBeg, selfPage ? selfLane : 0);
-                        auto selfIndex = [&](uint32_t t) -> uint32_t
-                        {
-                            uint32_t const q = cPre + (t - cBeg);
-                            return (selfPage && q >= cb && q < ce) ? q - cb : 0xffffffffu;
-                        };
                         cullChunk<V4, T, PAIRMAX>(
-                            A, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(A.t), supT, R2g, c.lists.list, cap, countOnly);
+                            A, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
                         if(twoChunks)
                             cullChunk<V4, T, PAIRMAX>(
-                                Bc, sNX, sNY, sNZ, sH, sEnt, m, selfIndex(Bc.t), supT, R2g, c.lists.list, cap,
-                                countOnly);
+                                Bc, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                        cand += uint64_t(m) * nTargets;
                     }
-                    cand += uint64_t(total) * (min(32u, tEnd - tc) + (twoChunks ? min(32u, tEnd - tc - 32) : 0u));
+                    }
+                    if(countOnly)
+                    {
+                        // full chunks' masks counted each target's own entry once
+                        if(A.act && A.S == 1)
+                            --A.nl;
+                        if(Bc.act && Bc.S == 1)
+                            --Bc.nl;
                     }
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
