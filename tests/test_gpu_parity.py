@@ -145,9 +145,9 @@ def test_density_and_pairs_match_oracle(oracle, kernel, prec, cull, vary):
 @pytest.mark.parametrize("h_lo,n", [(0.25, 6000), (0.4, 4000)])
 def test_two_level_grid_pairs_match_oracle(oracle, kernel, prec, h_lo, n):
     """Smoothing lengths spanning 4x and 2.5x under the pair-max cull: the box
-    runs two cell levels with 3- or 4-way splits of the level-0 cells (the
-    oracle searches one level); the accepted pair sets are the same and the
-    densities agree to round-off."""
+    runs two cell levels, the level-0 cells split in two along the axes their
+    edge allows (the oracle searches one level); the accepted pair sets are the
+    same and the densities agree to round-off."""
     p, boxes, sp = _cloud(kernel, prec, n=n, cull=abi.CULL_PAIR_MAX, vary_h=True, h_lo=h_lo)
     ctx = _ctx(p, boxes, sp)
     ctx.density()
@@ -159,6 +159,71 @@ def test_two_level_grid_pairs_match_oracle(oracle, kernel, prec, h_lo, n):
     orc.density()
     rel = np.max(np.abs(got.density / orc.s.density - 1.0))
     assert rel <= TOL[prec]["rho"], rel
+
+
+@pytest.mark.parametrize("kernel", [CUBIC, WENDLAND])
+@pytest.mark.parametrize("prec", PRECS)
+def test_pairs_at_the_cull_radius_match_oracle(oracle, kernel, prec):
+    """A dyadic lattice (spacing 1/16, 10 points per periodic axis) whose cull
+    radius is exactly two spacings.  The cell edge is the radius widened by
+    2^-20, so each axis holds four cells of 2.5 spacings (5/32): cell corners,
+    cell-relative positions and every distance are exact.  Pairs at r = R and
+    beyond are rejected (strict r^2 < R^2) and the 26 offsets with
+    i^2 + j^2 + k^2 <= 3 are accepted, through the staging box test, in cells
+    of 8 to 27 targets (short and full chunks)."""
+    dx = 1.0 / 16.0
+    g = np.arange(10) * dx
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    n = X.size
+    s = abi.Species(n)
+    s.pos[:] = np.stack([X.ravel(), Y.ravel(), Z.ravel()])
+    s.h[:] = dx  # support 2h = 2 dx
+    s.mass[:] = 1e-3
+    s.u[:] = 1.0
+    p = abi.default_params(kernel=kernel, precision=prec, h0=dx)
+    boxes = [abi.make_box((0, 0, 0), (10 * dx,) * 3, (1, 1, 1))]
+    sp = {abi.SPECIES_DEFAULT: s}
+    ctx = _ctx(p, boxes, sp)
+    ctx.density()
+    got = ctx.get_species(abi.SPECIES_DEFAULT)
+    counts = ctx.neighbour_counts(abi.SPECIES_DEFAULT)
+    assert np.all(counts == 26)
+    orc = _oracle(oracle, p, boxes, sp)
+    ocounts, _ = orc.neighbour_counts(fp32_geometry=(prec == abi.PREC_FP32_COMP))
+    assert np.array_equal(counts, ocounts)
+    orc.density()
+    rel = np.max(np.abs(got.density / orc.s.density - 1.0))
+    assert rel <= TOL[prec]["rho"], rel
+    ctx.close()
+
+
+@pytest.mark.parametrize("kernel", [CUBIC, WENDLAND])
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("cull,vary", [(abi.CULL_GLOBAL, False), (abi.CULL_PAIR_MAX, True)])
+def test_dense_cluster_matches_oracle(oracle, kernel, prec, cull, vary):
+    """A tenth of the box's particles in a ball of radius 0.04 inside a uniform
+    cloud: the cluster's cells hold hundreds of targets, so a cell runs many
+    64-target chunk pairs, each with its own staging box, plus a short tail
+    chunk; the accepted pair sets are the oracle's and the densities agree."""
+    p, boxes, sp = _cloud(kernel, prec, n=3000, cull=cull, vary_h=vary)
+    s = sp[abi.SPECIES_DEFAULT]
+    rng = np.random.default_rng(11)
+    k = 300
+    d = rng.normal(size=(3, k))
+    d *= 0.04 * rng.uniform(0.0, 1.0, k) ** (1 / 3) / np.linalg.norm(d, axis=0)
+    s.pos[:, :k] = 0.5 + d
+    ctx = _ctx(p, boxes, sp)
+    ctx.density()
+    got = ctx.get_species(abi.SPECIES_DEFAULT)
+    counts = ctx.neighbour_counts(abi.SPECIES_DEFAULT)
+    assert counts[:k].min() >= k - 1  # the whole cluster is in every member's reach
+    orc = _oracle(oracle, p, boxes, sp)
+    ocounts, _ = orc.neighbour_counts(fp32_geometry=(prec == abi.PREC_FP32_COMP))
+    assert np.array_equal(counts, ocounts)
+    orc.density()
+    rel = np.max(np.abs(got.density / orc.s.density - 1.0))
+    assert rel <= TOL[prec]["rho"], rel
+    ctx.close()
 
 
 @pytest.mark.parametrize("kernel", [CUBIC, QUINTIC, WENDLAND])
