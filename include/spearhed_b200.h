@@ -37,7 +37,7 @@ enum
     SPH_ERR_INVALID = 1,       /* bad argument (null pointer, bad enum, n < 0 ...)          */
     SPH_ERR_CUDA = 2,          /* a CUDA runtime call failed                                */
     SPH_ERR_NOMEM = 3,         /* device allocation failed                                  */
-    SPH_ERR_OUTSIDE = 4,       /* a particle left a non-periodic box                        */
+    SPH_ERR_OUTSIDE = 4,       /* a particle outside its box (see SphBox)                    */
     SPH_ERR_NONFINITE = 5,     /* NaN/Inf position, h <= 0 or mass <= 0 in the input        */
     SPH_ERR_OVERFLOW = 6,      /* a neighbour list exceeded its capacity (retry is automatic) */
     SPH_ERR_STATE = 7,         /* call out of order (e.g. hydro before density)             */
@@ -124,7 +124,9 @@ typedef struct SphParams
 } SphParams;
 
 /* A particle box: the reference's fluid/wall domain (an AABB, spmacc/particles/regions/AABB.hpp:38-127).
- * Particles must stay inside [lo, hi) along non-periodic axes. */
+ * Particles must lie inside [lo, hi] on every axis when they are set.  Along a periodic axis the
+ * drift wraps movable particles back into [lo, hi) every step; a particle that leaves a
+ * non-periodic axis, or lies outside a periodic one it was not wrapped on, is SPH_ERR_OUTSIDE. */
 typedef struct SphBox
 {
     double lo[3];

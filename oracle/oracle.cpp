@@ -369,7 +369,8 @@ namespace orc
             {
                 if(!std::isfinite(x[a]))
                     return SPH_ERR_NONFINITE;
-                if(!g.periodic[a] && (x[a] < g.lo[a] || x[a] > g.lo[a] + g.L[a]))
+                // every axis (the drift has wrapped movable particles on periodic ones)
+                if(x[a] < g.lo[a] || x[a] > g.lo[a] + g.L[a])
                     return SPH_ERR_OUTSIDE;
             }
             s.cx[i] = cellCoord(g, 0, x[0]);

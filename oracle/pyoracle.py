@@ -30,10 +30,20 @@ def build(ref: bool = True):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
+def _stale() -> bool:
+    """The library is missing or older than a source it is built from."""
+    if not os.path.exists(ORACLE_SO):
+        return True
+    built = os.path.getmtime(ORACLE_SO)
+    srcs = [os.path.join(HERE, "oracle.cpp"), os.path.join(HERE, "Makefile"),
+            os.path.join(os.path.dirname(HERE), "include", "spearhed_b200.h")]
+    return any(os.path.exists(f) and os.path.getmtime(f) > built for f in srcs)
+
+
 def orc():
     global _ORC
     if _ORC is None:
-        if not os.path.exists(ORACLE_SO):
+        if _stale():
             build(ref=False)
         L = C.CDLL(ORACLE_SO)
         P = C.POINTER

@@ -477,8 +477,11 @@ int sph_ctx::layout()
                 double const x = s.col[cX + a][i];
                 if(!std::isfinite(x))
                     return fail(SPH_ERR_NONFINITE, "non-finite position in the input");
-                if(!B.periodic[a] && (x < B.lo[a] || x > B.hi[a]))
-                    return fail(SPH_ERR_OUTSIDE, "particle outside a non-periodic box axis");
+                // periodic axes too: the cell search covers [lo, hi]; the drift
+                // wraps movable particles back into it every step
+                if(x < B.lo[a] || x > B.hi[a])
+                    return fail(SPH_ERR_OUTSIDE, B.periodic[a] ? "particle outside its box along a periodic axis"
+                                                              : "particle outside a non-periodic box axis");
             }
             if(!(s.col[cH][i] > 0.0) || !std::isfinite(s.col[cH][i]))
                 return fail(SPH_ERR_NONFINITE, "smoothing length must be positive and finite");
@@ -893,7 +896,8 @@ int sph_ctx::checkStatus(char const* where)
     if(stat[sph::kStatOutside])
         return fail(
             SPH_ERR_OUTSIDE,
-            std::string(where) + ": " + std::to_string(stat[sph::kStatOutside]) + " particles left a non-periodic box");
+            std::string(where) + ": " + std::to_string(stat[sph::kStatOutside])
+                + " particles outside their box (a non-periodic axis, or a periodic one they were not wrapped on)");
     if(stat[sph::kStatOverflow])
         return fail(
             SPH_ERR_OVERFLOW,

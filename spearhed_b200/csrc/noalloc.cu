@@ -107,7 +107,7 @@ namespace
         double const pos[3] = {x[p], y[p], z[p]};
         bool bad = false;
         for(int a = 0; a < 3; ++a)
-            bad = bad || !isfinite(pos[a]) || (!B.periodic[a] && (pos[a] < B.lo[a] || pos[a] > B.lo[a] + B.L[a]));
+            bad = bad || !isfinite(pos[a]) || pos[a] < B.lo[a] || pos[a] > B.lo[a] + B.L[a]; // every axis
         if(bad)
             atomicAdd(&status[0], 1u);
         int const cx = sph::cellCoord(B, 0, isfinite(pos[0]) ? pos[0] : B.lo[0]);
@@ -471,7 +471,7 @@ int sph_density_noalloc(
     if(bad)
         return failNoAlloc(
             SPH_ERR_OUTSIDE,
-            "sph_density_noalloc: " + std::to_string(bad) + " particles non-finite or outside a non-periodic axis");
+            "sph_density_noalloc: " + std::to_string(bad) + " particles non-finite or outside the box");
     return SPH_OK;
 }
 }

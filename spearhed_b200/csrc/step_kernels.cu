@@ -57,10 +57,13 @@ namespace sph
             }
             else
             {
+                // every axis: a drifted particle was wrapped on its periodic axes;
+                // one that was not (frozen, a density-only call, the same-size
+                // species path) must lie in [lo, hi] for the cell search
                 bool outside = false;
 #pragma unroll
                 for(int a = 0; a < 3; ++a)
-                    if(!B.periodic[a] && (x[a] < B.lo[a] || x[a] > B.lo[a] + B.L[a]))
+                    if(x[a] < B.lo[a] || x[a] > B.lo[a] + B.L[a])
                         outside = true;
                 if(outside)
                     atomicAdd(&c.status[kStatOutside], 1u);

@@ -3,7 +3,7 @@ words (no GPU fault is involved: the kernels count bad particles, the host
 reads the counts and returns a status).
 
 - set-up: non-finite positions, h <= 0, non-positive source masses and
-  particles outside a non-periodic box axis are refused;
+  particles outside their box (on any axis, periodic ones included) are refused;
 - stepping: a particle driven out of a non-periodic box is reported by the
   drift kernel (SPH_ERR_OUTSIDE);
 - the same-size fast path of sph_set_species checks h and masses on the device.
@@ -60,6 +60,40 @@ def test_particle_leaving_a_closed_box_is_reported():
     ctx = _ctx(s)
     assert _code(lambda: ctx.step(2, 1e-3)) == abi.SPH_ERR_OUTSIDE
     ctx.close()
+
+
+def test_outside_a_periodic_axis_is_refused_at_set_up():
+    s = _cloud()
+    s.pos[0, 7] = 1.5  # periodic axis, but outside [lo, hi]: the cell search would miss pairs
+    ctx = _ctx(s, periodic=(1, 1, 1))
+    assert _code(lambda: ctx.step(1)) == abi.SPH_ERR_OUTSIDE
+    ctx.close()
+
+
+def test_upper_face_of_a_periodic_axis_is_the_lower_face():
+    """x = hi is accepted on a periodic axis and is the same place as x = lo:
+    every density agrees to round-off (the positions relative to the cells differ)."""
+    import spearhed_b200 as sb
+    rng = np.random.default_rng(4)
+    n = 600
+    s = abi.Species(n)
+    s.pos[:] = rng.uniform(0.0, 1.0, size=(3, n))
+    s.pos[0, :40] = 0.0
+    s.h[:] = 0.08
+    s.mass[:] = 1e-3
+    s.u[:] = 1.0
+    p = abi.default_params(h0=0.08, precision=abi.PREC_FP64)
+    box = [abi.make_box((0, 0, 0), (1, 1, 1), (1, 1, 1))]
+    rho = []
+    for x0 in (0.0, 1.0):
+        t = s.copy()
+        t.pos[0, :40] = x0
+        ctx = sb.Context(p, box)
+        ctx.set_species(abi.SPECIES_DEFAULT, t)
+        ctx.density()
+        rho.append(ctx.get_species(abi.SPECIES_DEFAULT).density.copy())
+        ctx.close()
+    assert np.max(np.abs(rho[1] / rho[0] - 1.0)) < 1e-12
 
 
 def test_periodic_axis_wraps_instead():

@@ -167,6 +167,19 @@ def test_hydro_two_particles_at_rest(oracle):
     assert np.allclose(sysm.s.dudt, 0.0, atol=1e-6)
 
 
+def test_position_outside_a_periodic_axis_is_refused(oracle):
+    """The cell search covers [lo, hi] on every axis: a particle outside it is
+    SPH_ERR_OUTSIDE on periodic axes too, while x = hi is accepted."""
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(0.0, 1.0, size=(3, 200))
+    box = abi.make_box((0, 0, 0), (1, 1, 1), (1, 1, 1))
+    pos[0, 3] = 1.0
+    _system(oracle, pos, 1e-3, 0.08, 0.0, 1.0, box=box).density()
+    pos[0, 3] = 1.5
+    with pytest.raises(RuntimeError, match=f"oracle error {abi.SPH_ERR_OUTSIDE}"):
+        _system(oracle, pos, 1e-3, 0.08, 0.0, 1.0, box=box).density()
+
+
 # ---- the oracle's FP64 passes are the reference functors, bit for bit ----
 def _random_cloud(oracle, kernel, n=1500, seed=11, periodic=(0, 1, 0)):
     rng = np.random.default_rng(seed)
