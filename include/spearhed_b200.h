@@ -173,7 +173,8 @@ typedef struct SphDiag
     int64_t steps;         /* steps taken by this context                                   */
     int64_t n_targets;     /* particles in the sums                                         */
     double pairs_total;    /* accepted ordered pairs summed over every step's neighbour build */
-    double candidates;     /* (target, staged source) pairs the cull tested in the last build */
+    double candidates;     /* (target, staged source) pairs the cull tested in the last build
+                              (sources that passed the staging box test)                     */
     int64_t replays;       /* step calls this context re-ran after a neighbour-list overflow */
     int64_t list_capacity; /* neighbour-list entries per particle currently allocated      */
 } SphDiag;
