@@ -356,14 +356,28 @@ int sph_sc_cell_counts_f32(const float* lo, const float* hi, float spacing, uint
  * entry point takes caller-owned DEVICE arrays (positions, mass, h; length n) and
  * writes rho (device, length n, input order); its scratch is one fixed 32 MiB
  * device array inside this library (held on every GPU that loads it until the
- * process exits).  Limits: n <= 262144 particles, <= 262144 cells, one box,
- * params->cull == SPH_CULL_GLOBAL; larger inputs return SPH_ERR_INVALID.
+ * process exits).  Limits: n <= 262144 particles, <= 262144 cells, one box.
  * Every Default-species rule applies (all particles are targets and sources).
  * The work runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
- * the call returns after it finished.  Calls share the scratch array: calls
- * whose device work overlaps (other threads or unordered streams) race and give
- * wrong results.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture. */
+ * the call synchronizes that stream before it returns.  Calls share the scratch
+ * array: calls whose device work overlaps (other threads or unordered streams)
+ * race and give wrong results.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) and keeps it for the process; make that first
+ * call before any stream capture, and make no call on a device after
+ * cudaDeviceReset() on it.
+ * Returns:
+ *   SPH_OK               rho written;
+ *   SPH_ERR_INVALID      a null pointer, bad enums or h0, an empty or non-finite box,
+ *                        n or the cell count above the limits, or a layout that does
+ *                        not fit the scratch array (nothing launched);
+ *   SPH_ERR_UNSUPPORTED  params->cull == SPH_CULL_PAIR_MAX, or a periodic axis
+ *                        shorter than the cull radius (nothing launched);
+ *   SPH_ERR_NONFINITE    a non-finite position, or a mass or h that is not finite
+ *                        and positive (found on the device; rho must not be used);
+ *   SPH_ERR_OUTSIDE      a finite position outside [lo, hi] on any axis, periodic
+ *                        axes included (found on the device; rho must not be used);
+ *   SPH_ERR_CUDA         no current device, the scratch address lookup failed, or
+ *                        a CUDA call or launch of this entry point failed. */
 int sph_density_noalloc(const SphParams* params, const SphBox* box, int64_t n, const double* x, const double* y,
                         const double* z, const double* mass, const double* h, double* rho, void* stream);
 

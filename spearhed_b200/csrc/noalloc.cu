@@ -24,7 +24,17 @@
 //
 // Set-up: the first call on each device looks up the array's device address
 // with cudaGetSymbolAddress while that device is current; that first call
-// should be made before any stream capture begins.
+// should be made before any stream capture begins.  The address is kept for
+// the life of the process, so the entry point must not be called on a device
+// after cudaDeviceReset() on it (the reset unloads the module that holds the
+// array; a later call would write through the stale address).
+//
+// Inputs are checked on the device as in sph_set_species: a non-finite
+// position, or a mass or h that is not finite and positive, returns
+// SPH_ERR_NONFINITE; a finite position outside the box returns SPH_ERR_OUTSIDE.
+// Those inputs are found by the same launch sequence that computes rho, so
+// on either return rho holds values that must not be used.  Every call waits
+// for its own work on `stream` before it returns.
 #include "sph_launch.hpp"
 
 #include <cmath>
@@ -90,12 +100,17 @@ namespace
     constexpr int kWarps = 4;
 
     //! Cell key of every particle (input order); one box, every particle a target.
+    //! status[0] counts finite positions outside the box (on every axis,
+    //! periodic ones included), status[1] non-finite positions and masses or
+    //! smoothing lengths that are not finite and positive.
     __global__ void kKeysInput(
         sph::BoxDev const* __restrict__ box,
         uint32_t n,
         double const* __restrict__ x,
         double const* __restrict__ y,
         double const* __restrict__ z,
+        double const* __restrict__ m,
+        double const* __restrict__ h,
         uint32_t* __restrict__ keys,
         uint32_t* __restrict__ vals,
         uint32_t* __restrict__ status)
@@ -105,10 +120,17 @@ namespace
             return;
         sph::BoxDev const& B = *box;
         double const pos[3] = {x[p], y[p], z[p]};
-        bool bad = false;
+        double const mp = m[p], hp = h[p];
+        bool nonfinite = !(isfinite(mp) && mp > 0.0) || !(isfinite(hp) && hp > 0.0);
+        bool outside = false;
         for(int a = 0; a < 3; ++a)
-            bad = bad || !isfinite(pos[a]) || pos[a] < B.lo[a] || pos[a] > B.lo[a] + B.L[a]; // every axis
-        if(bad)
+        {
+            nonfinite = nonfinite || !isfinite(pos[a]);
+            outside = outside || pos[a] < B.lo[a] || pos[a] > B.lo[a] + B.L[a];
+        }
+        if(nonfinite)
+            atomicAdd(&status[1], 1u);
+        else if(outside)
             atomicAdd(&status[0], 1u);
         int const cx = sph::cellCoord(B, 0, isfinite(pos[0]) ? pos[0] : B.lo[0]);
         int const cy = sph::cellCoord(B, 1, isfinite(pos[1]) ? pos[1] : B.lo[1]);
@@ -181,7 +203,7 @@ namespace
     //! the sorted records.  Same acceptance rule and summation order as the
     //! list-based kernel; the FP32 variant folds blocks of 8 accepted terms
     //! into a TwoSum-compensated sum.  rho is written in input order.
-    template<int K, typename V4, typename T, bool PAIRMAX>
+    template<int K, typename V4, typename T>
     __global__ void __launch_bounds__(kWarps * 32) kDensityInline(
         sph::BoxDev const* __restrict__ box,
         sph::Cells cells,
@@ -247,14 +269,7 @@ namespace
                         T const dx = own.x - qx, dy = own.y - qy, dz = own.z - qz;
                         // unfused, x then y then z: the acceptance test of the list-based kernel
                         T const r2 = addRn(addRn(mulRn(dx, dx), mulRn(dy, dy)), mulRn(dz, dz));
-                        T R2 = R2g;
-                        if constexpr(PAIRMAX)
-                        {
-                            T const hj = hc[j];
-                            T const R = mulRn(sup, hi > hj ? hi : hj);
-                            R2 = mulRn(R, R);
-                        }
-                        if(r2 < R2)
+                        if(r2 < R2g)
                         {
                             T const r = r2 > T(0) ? r2 * (T(1) / sqrt(r2)) : T(0);
                             T const term = pj.w * sph::kernelW<K, T>(r, hk);
@@ -300,10 +315,8 @@ namespace
     {
         uint32_t blocks = (cells.ncells + kWarps - 1) / kWarps;
         blocks = blocks > 148u * 32u ? 148u * 32u : blocks;
-        if(p.cull == SPH_CULL_PAIR_MAX)
-            kDensityInline<K, V4, T, true><<<blocks, kWarps * 32, 0, s>>>(box, cells, perm, pm, hc, p.h0, rho);
-        else
-            kDensityInline<K, V4, T, false><<<blocks, kWarps * 32, 0, s>>>(box, cells, perm, pm, hc, p.h0, rho);
+        // the global cull radius only: pair-max calls are refused before any launch
+        kDensityInline<K, V4, T><<<blocks, kWarps * 32, 0, s>>>(box, cells, perm, pm, hc, p.h0, rho);
         sph::countLaunches(1);
     }
 
@@ -430,48 +443,75 @@ int sph_density_noalloc(
             "sph_density_noalloc: needs " + std::to_string(cv.used) + " bytes of scratch, the fixed array holds "
                 + std::to_string(kScratchBytes));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // A launch error left pending by earlier, unrelated work on this thread
+    // would otherwise be reported as this call's failure: clear it first.
+    (void)cudaGetLastError();
     // Everything below is stream-ordered; nothing that must start at zero is
     // assumed to be zero from an earlier call.
     if(cudaMemcpyAsync(dBox, &bd, sizeof(bd), cudaMemcpyHostToDevice, s) != cudaSuccess
        || cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), s) != cudaSuccess)
         return failNoAlloc(SPH_ERR_CUDA, "sph_density_noalloc: stream operation failed");
+    auto launched = [](char const* what) -> int
+    {
+        // launch configuration errors and failed memsets of the launchers
+        cudaError_t const e = cudaGetLastError();
+        if(e == cudaSuccess)
+            return SPH_OK;
+        return failNoAlloc(SPH_ERR_CUDA, std::string("sph_density_noalloc: ") + what + ": " + cudaGetErrorString(e));
+    };
     unsigned const g = (nn + kThreads - 1) / kThreads;
-    kKeysInput<<<g, kThreads, 0, s>>>(dBox, nn, x, y, z, keysA, valsA, status);
+    kKeysInput<<<g, kThreads, 0, s>>>(dBox, nn, x, y, z, mass, h, keysA, valsA, status);
     sph::countLaunches(1);
+    if((st = launched("cell keys")))
+        return st;
     int bits = 1;
     while((uint64_t(1) << bits) <= ncells * 2)
         ++bits;
     bool const inB = sph::radixSortPairs(keysA, valsA, keysB, valsB, nn, bits, sortScr, s);
+    if((st = launched("radix sort")))
+        return st;
     uint32_t const* keys = inB ? keysB : keysA;
     uint32_t const* perm = inB ? valsB : valsA;
     sph::DevCtx dc{};
     dc.n = nn;
     dc.cells = cells;
     sph::launchCellRanges(dc, keys, s); // clears start/mid/end, then fills them
+    if((st = launched("cell ranges")))
+        return st;
     if(fp64)
     {
         kPackSorted<sph::D4, double><<<g, kThreads, 0, s>>>(dBox, nn, perm, x, y, z, mass, h, pm64, hc64);
         sph::countLaunches(1);
+        if((st = launched("packing")))
+            return st;
         launchInlineK<sph::D4, double>(dBox, cells, perm, pm64, hc64, p, rho, s);
     }
     else
     {
         kPackSorted<float4, float><<<g, kThreads, 0, s>>>(dBox, nn, perm, x, y, z, mass, h, pm32, hc32);
         sph::countLaunches(1);
+        if((st = launched("packing")))
+            return st;
         launchInlineK<float4, float>(dBox, cells, perm, pm32, hc32, p, rho, s);
     }
-    uint32_t bad = 0;
-    cudaError_t e = cudaMemcpyAsync(&bad, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if((st = launched("density")))
+        return st;
+    // Bad inputs are only known after the work ran, so the density kernel is
+    // told nothing; rho is written but must not be used on an error return.
+    uint32_t bad[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(bad, status, sizeof(bad), cudaMemcpyDeviceToHost, s);
     if(e == cudaSuccess)
         e = cudaStreamSynchronize(s);
-    if(e == cudaSuccess)
-        e = cudaGetLastError();
     if(e != cudaSuccess)
         return failNoAlloc(SPH_ERR_CUDA, std::string("sph_density_noalloc: ") + cudaGetErrorString(e));
-    if(bad)
+    if(bad[1])
         return failNoAlloc(
-            SPH_ERR_OUTSIDE,
-            "sph_density_noalloc: " + std::to_string(bad) + " particles non-finite or outside the box");
+            SPH_ERR_NONFINITE,
+            "sph_density_noalloc: " + std::to_string(bad[1])
+                + " particles with a non-finite position or a mass or h that is not finite and positive");
+    if(bad[0])
+        return failNoAlloc(
+            SPH_ERR_OUTSIDE, "sph_density_noalloc: " + std::to_string(bad[0]) + " particles outside the box");
     return SPH_OK;
 }
 }
