@@ -23,11 +23,14 @@ _ORC = None
 _REF = None
 
 
-def build(ref: bool = True):
-    """Compile the oracle (and the reference harness when the checkout exists)."""
+def build(ref: bool = True, ref_root: str | None = None):
+    """Compile the oracle, and the reference harness when a reference checkout
+    is given (``ref_root`` or the REF_ROOT environment variable) and exists;
+    without one the harness is left as it is (prebuilt, or absent)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(os.environ.get("REF_ROOT", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    root = ref_root or os.environ.get("REF_ROOT")
+    if ref and root and os.path.isdir(root):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={root}"], check=True)
 
 
 def _stale() -> bool:

@@ -1,15 +1,8 @@
-/* Host-only stand-in for the reference's alpaka-backed math functions. */
+/* Host-only stand-in for the reference's alpaka-backed math functions
+ * (packages/pmacc/include/pmacc/math/functions/Abs.hpp): abs. */
 #pragma once
-#include <cmath>
+#include "Root.hpp"
 namespace pmacc::math
 {
     using std::abs;
-    using std::pow;
-    using std::sqrt;
-    //! 1/sqrt(x) in the argument's own precision (the oracle's rsqrt, see oracle.hpp).
-    template<typename T>
-    inline T rsqrt(T x)
-    {
-        return T(1) / std::sqrt(x);
-    }
 } // namespace pmacc::math

@@ -10,6 +10,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs through the C ABI")
+    config.addinivalue_line("markers", "fullsize: a benchmark configuration at its full size (minutes; also gpu)")
 
 
 @pytest.fixture(scope="session")

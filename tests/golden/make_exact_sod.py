@@ -5,7 +5,9 @@ share/spearhed/ValidationSetups/SodShockTube/validate_sod.py (its plotting
 import, matplotlib, is not installed here and is not used by exact_sod, so a
 bare stand-in module satisfies the import).  Run from the repository root:
 
-    python tests/golden/make_exact_sod.py [REFERENCE_ROOT]
+    python tests/golden/make_exact_sod.py REFERENCE_ROOT
+
+(REFERENCE_ROOT may also come from the REF_ROOT environment variable.)
 """
 import importlib.util
 import os
@@ -14,7 +16,9 @@ import types
 
 import numpy as np
 
-ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+if not ref_root:
+    sys.exit("usage: make_exact_sod.py REFERENCE_ROOT (or set REF_ROOT): the reference checkout to import from")
 path = os.path.join(ref_root, "share/spearhed/ValidationSetups/SodShockTube/validate_sod.py")
 mpl = types.ModuleType("matplotlib")
 mpl.use = lambda *a, **k: None
