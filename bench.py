@@ -1,14 +1,18 @@
-"""Benchmark: SPH pair-interactions/s of the Orszag-Tang SPMHD step on B200.
+"""Benchmark: SPH pair-interactions/s of the batched Brio-Wu MHD ensemble on B200.
 
-Workload (default): Orszag-Tang vortex, thin periodic slab [0,1]^2 x [0,1/128],
-512 x 512 x 4 lattice = 1,048,576 equal-mass particles, Wendland C2 kernel
-(h = 1.45 spacing, ~100 neighbours), artificial viscosity, SPMHD with Dedner
-cleaning and the tensile correction, CFL time step; synthetic initial
-conditions of that shape (no dataset is involved).
+Workload (default): 512 independent 3D Brio-Wu MHD shock tubes (gamma 2,
+Bx 0.75, By +1 / -1, rho 1 / 0.125, P 1 / 0.1), particle counts drawn
+log-uniform in [4k, 256k] from seed 5 (31.3 M particles in all), cubic spline,
+artificial viscosity, SPMHD with Dedner cleaning and the tensile correction,
+adaptive h, a CFL time step per box; synthetic initial conditions of that
+shape (no dataset is involved).  Every box lives in one context: one sort and
+one launch of each kernel serve all 512 boxes, the density pass pulls
+(box, cell) work items from a device queue, and the timed steps replay CUDA
+graphs.  --workload selects the single-box configurations instead.
 
-A step is one full runOneStep: drift, cell keys, radix sort, permute, neighbour
-build + density, fused hydro/AV + SPMHD/Dedner force pass, kick, FP64
-conserved-quantity reductions and the CFL minimum.
+A step is one full runOneStep of every box: drift, cell keys, radix sort,
+permute, neighbour build + density, fused hydro/AV + SPMHD/Dedner force pass,
+kick, FP64 conserved-quantity reductions and the per-box CFL minimum.
 
 value  = accepted ordered pairs per pass x 3 logical pair passes (density,
          hydro/AV, SPMHD/Dedner) per step x steps / device time of those steps
@@ -16,13 +20,20 @@ value  = accepted ordered pairs per pass x 3 logical pair passes (density,
 e2e    = the same metric through the C ABI with pinned host buffers: every
          step copies the state in (sph_set_species), runs sph_step(1) and copies
          the state out (sph_get_species), all inside the timed region.
-The FP64-plain kernel on the same GPU and workload is reported beside it
-(fp64_plain), with the FP32 run's errors against it after one step.
+fp64_plain = the FP64-plain kernels on the same GPU: the same batched ensemble
+         (one context), and the FP64 single-box step looped over the boxes (one
+         context per box, the reference's one-simulation-per-run shape); the
+         FP32 run's errors against the FP64 run after one step beside them.
+reference_physics = the same 512 boxes under the reference's own step
+         (inviscid hydro, one constant h per box, constant dt, no periodic
+         images, 2 pair passes), FP32 on the GPU: the pair set and physics the
+         reference arm times on the CPU, so the two read like for like.
 
---impl reference times the reference's own CPU path for this step (its density
-and hydro functors compiled from the reference sources, oracle/_ref, driven by
-a restatement of its region/frame pair engine) on the host cores, or the
-oracle port when oracle/_ref is absent.
+--impl reference times the reference's own CPU path for that step (its
+DensityInitSelf/AccumulateDensity and HydroInteraction functors compiled from
+the reference sources, oracle/_ref, driven by a restatement of its
+region/frame pair engine) over a seeded random sample of the same boxes on
+all host cores, or the oracle port when oracle/_ref is absent.
 """
 from __future__ import annotations
 
@@ -45,14 +56,14 @@ METRIC = "SPH pair-interactions/s: FP32-mixed vs FP64 plain on 1 B200 at stated 
 UNIT = "pair-interactions/s"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nx", type=int, default=512)
-    ap.add_argument("--nz", type=int, default=4)
+    ap.add_argument("--nx", type=int, default=512, help="orszag_tang only: lattice edge")
+    ap.add_argument("--nz", type=int, default=4, help="orszag_tang only: lattice layers")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--fp64-steps", type=int, default=5)
     ap.add_argument("--eager", dest="graph", action="store_false",
@@ -61,12 +72,18 @@ def parse():
     ap.set_defaults(graph=True)
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no sph_autotune)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="orszag_tang",
-                    choices=["orszag_tang", "kelvin_helmholtz", "mhd_rotor", "brio_wu_ensemble", "sod_small"],
-                    help="orszag_tang (the headline) or one of the other configurations")
-    ap.add_argument("--fp64-boxes", type=int, default=8,
-                    help="ensemble only: boxes of the FP64 single-box loop sample")
-    return ap.parse_args()
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the reference-physics and Orszag-Tang legs of the ensemble line")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="pass time of the CPU baseline's box sample")
+    ap.add_argument("--workload", default="brio_wu_ensemble",
+                    choices=["brio_wu_ensemble", "orszag_tang", "kelvin_helmholtz", "mhd_rotor", "sod_small"],
+                    help="brio_wu_ensemble (the headline: the largest single-GPU configuration) or a single box")
+    ap.add_argument("--fp64-boxes", type=int, default=0,
+                    help="ensemble only: boxes of the FP64 single-box loop (0 = every box of this rank)")
+    ap.add_argument("--fp64-loop-steps", type=int, default=3,
+                    help="ensemble only: timed steps of each box in the FP64 single-box loop")
+    return ap.parse_args(argv)
 
 
 WORKLOADS = {
@@ -235,14 +252,27 @@ def pinned_species(src, fields):
     return s
 
 
+PROFILED = {
+    # workload -> (density summary, force summary) under profiles/
+    "orszag_tang": ("density_fp32_orszag_tang.txt", "force_mhd_fp32_orszag_tang.txt"),
+    "brio_wu_ensemble": ("density_fp32_brio_wu_ensemble.txt", "force_mhd_fp32_brio_wu_ensemble.txt"),
+}
+
+
 def profiled_config(args):
-    """True when this run is the configuration the committed ncu captures were
-    taken on (the default Orszag-Tang slab, 512 x 512 x 4)."""
-    return args.workload == "orszag_tang" and (args.nx, args.nz) == (512, 4)
+    """True when this run is a configuration a committed ncu summary covers
+    (the 512-box Brio-Wu ensemble, or the Orszag-Tang slab at 512 x 512 x 4)."""
+    if args.workload == "orszag_tang":
+        return (args.nx, args.nz) == (512, 4)
+    return args.workload in PROFILED
 
 
 def traffic_from_profiles(name):
-    """DRAM bytes per launch recorded from an ncu capture under profiles/ (or None)."""
+    """DRAM bytes per launch recorded from an ncu capture under profiles/ (or None).
+
+    The line ``dram_bytes_per_launch_full_workload: X`` holds the bytes of one
+    launch on the full workload, measured or scaled from a smaller capture of
+    the same kernel as the summary states."""
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
@@ -253,13 +283,6 @@ def traffic_from_profiles(name):
             except ValueError:
                 return None
     return None
-
-
-def warm_graphs(ctx):
-    """Capture, outside the timed region, the two-step graph the timed call
-    starts with; the capture steps run from a snapshot that is restored, so the
-    timed steps start from the state they would have started from anyway."""
-    ctx.prepare_graph()
 
 
 def hbm_view(kernel, peak_gbs):
@@ -281,9 +304,62 @@ def measured_peak(key):
 
 
 # ------------------------------------------------------- CPU baselines
+def reference_box_sample(limit_s=20.0, order_seed=11):
+    """The reference's CPU path over a seeded random sample of the ensemble's
+    boxes under the reference's own step: its DensityInitSelf/AccumulateDensity
+    and HydroInteraction functors (compiled from its headers, FP32) under its
+    region/frame engine (64-slot frames, regions of 4 x 4 x 4 left lattice
+    cells, AABB region search), cubic spline, one constant h per box (1.2 left
+    spacings) with the radius 2h, no periodic images; whole boxes in the
+    sample's order until `limit_s` of pass time.  Falls back to the oracle port
+    (oracle.cpp, FP64) when oracle/_ref was not built."""
+    from oracle import pyoracle
+    from spearhed_b200 import abi, setups
+    cores = os.cpu_count() or 1
+    sizes = setups.brio_wu_sizes()
+    order = np.random.default_rng(order_seed).permutation(len(sizes))
+    ref = pyoracle.ref()
+    use_ref = ref is not None and hasattr(ref, "ref_region_bench_f32")
+    pairs = secs = 0.0
+    done, parts = [], 0
+    for b in order:
+        w = setups.brio_wu_ensemble(precision=abi.PREC_FP32_COMP, reference_physics=True, boxes=[int(b)])
+        s = w.species[abi.SPECIES_DEFAULT]
+        box = w.boxes[0]
+        if use_ref:
+            side = 4.0 * w.params.h0 / 1.2  # regions of 4 x 4 x 4 left lattice cells: one 64-slot frame
+            r = pyoracle.region_bench(s, w.params, list(box.lo), list(box.hi), side, limit_s=1e30)
+            pairs += r["pairs_density"] + r["pairs_hydro"]
+            secs += r["seconds"]
+        else:
+            p = abi.SphParams.from_buffer_copy(w.params)
+            p.precision = abi.PREC_FP64
+            orc = pyoracle.System(p, [box], s.copy(), np.full(s.n, abi.ROLES_DEFAULT, dtype=np.uint8))
+            _, np_pairs = orc.neighbour_counts()
+            t0 = time.perf_counter()
+            orc.density()
+            orc.force()
+            secs += time.perf_counter() - t0
+            pairs += 2 * np_pairs
+        done.append(int(b))
+        parts += s.n
+        if secs >= limit_s:
+            break
+    kind = "reference" if use_ref else "port"
+    what = ("the reference's own DensityInitSelf/AccumulateDensity and HydroInteraction functors (compiled from "
+            "its headers, FP32) under its region/frame engine (64-slot frames, AABB region search)" if use_ref else
+            "the oracle port (oracle.cpp, FP64 density + inviscid hydro passes)")
+    return {"value": pairs / secs if secs > 0 else None, "unit": UNIT, "cores": cores, "kind": kind,
+            "seconds": secs, "pairs": pairs, "boxes": len(done), "particles": parts,
+            "sample": (f"{len(done)} of {len(sizes)} Brio-Wu boxes ({parts} particles, seeded random order, whole "
+                       f"boxes): {what}, cubic spline, one constant h per box (1.2 left spacings) and the radius "
+                       f"2h, no periodic images (the reference has none), 2 pair passes (density, hydro); "
+                       f"pair-interactions = accepted ordered pairs of both passes / their wall time")}
+
+
 def cpu_reference_sample(nx, nz, limit_s=20.0):
     """The reference's density + hydro functors (compiled from its sources) over
-    a sample of target frames of the same workload, driven by its region/frame
+    a sample of target frames of the Orszag-Tang slab, driven by its region/frame
     engine restated in oracle/ref_functors.cpp.  Falls back to the oracle port."""
     from oracle import pyoracle
     from spearhed_b200 import abi, setups
@@ -297,8 +373,6 @@ def cpu_reference_sample(nx, nz, limit_s=20.0):
         r = pyoracle.region_bench(s, w.params, list(box.lo), list(box.hi), side, limit_s=limit_s)
         r["cores"] = cores
         return r
-    # Oracle port: density + force of the full SPMHD step on a smaller slab of
-    # the same resolution (nx_sample^2 x nz), all host threads.
     nxs = 128
     ws = setups.orszag_tang(nx=nxs, nz=nz)
     ss = ws.species[abi.SPECIES_DEFAULT].copy()
@@ -319,12 +393,208 @@ def cpu_reference_sample(nx, nz, limit_s=20.0):
                       f"same spacing ({ss.n} particles), 3 logical pair passes per accepted pair"}
 
 
+# ------------------------------------------------------------ GPU legs
+def prepared_context(w, dev, args, tune=True):
+    """A context on `w` after the warm-up steps, with its launch shapes tuned
+    and the graph of the first timed call captured (all outside timing)."""
+    import torch
+
+    import spearhed_b200 as sb
+    w.params.device = dev
+    ctx = sb.context_for(w)
+    if args.graph:
+        ctx.use_graph(True)
+    ctx.step(args.warmup)
+    shapes = ctx.autotune(2) if (tune and not args.no_tune) else ctx.tuning()
+    if args.graph:
+        # the capture steps run from a snapshot that is restored, so the timed
+        # steps start from the state they would have started from anyway
+        ctx.prepare_graph()
+    torch.cuda.synchronize()
+    return ctx, shapes
+
+
+def timed_steps(ctx, steps, dev, L=None, barrier=None, clocks=False):
+    """Device time, pairs and per-stage times of `steps` steps of `ctx`."""
+    import torch
+    d0 = ctx.reduce()
+    if barrier:
+        barrier()
+    torch.cuda.synchronize()
+    l0 = L.sphx_launch_count() if L is not None else 0
+    clk = ClockSampler(dev) if clocks else None
+    if clk:
+        clk.__enter__()
+    ctx.step(steps)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    launches = (L.sphx_launch_count() - l0) if L is not None else None
+    if barrier:
+        barrier()
+    tm = ctx.timings()  # [build, density, force, kick, whole] ms over the timed steps
+    d1 = ctx.reduce()
+    return {"ms": tm[4], "pairs": d1["pairs_total"] - d0["pairs_total"], "stages": tm,
+            "candidates": d1["candidates"], "replays": int(d1["replays"] - d0["replays"]),
+            "launches": launches, "clocks": clk.summary() if clk else None}
+
+
+def stage_dict(tm, steps):
+    return {"sort_permute": tm[0] / steps, "density": tm[1] / steps, "force": tm[2] / steps,
+            "kick_reduce": tm[3] / steps}
+
+
+def fp64_box_loop(args, dev, passes, global_boxes):
+    """The FP64-plain single-box step looped over the ensemble's boxes: one
+    context per box (the reference's one-simulation-per-run shape), each after
+    --warmup steps and a captured graph, --fp64-loop-steps timed steps; the
+    device times are summed.  Returns (pair-interactions/s, summed timings,
+    boxes, steps per box)."""
+    import spearhed_b200 as sb
+    from spearhed_b200 import abi, setups
+    sizes = setups.brio_wu_sizes()
+    boxes = list(global_boxes)
+    if args.fp64_boxes and args.fp64_boxes < len(boxes):
+        pick = np.linspace(0, len(boxes) - 1, args.fp64_boxes).astype(int)
+        boxes = [boxes[i] for i in pick]
+    pairs = 0.0
+    tm = [0.0] * 5
+    for b in boxes:
+        p, box, s = setups.brio_wu_box(int(sizes[b]), precision=abi.PREC_FP64)
+        p.device = dev
+        c = sb.Context(p, [box])
+        c.set_species(abi.SPECIES_DEFAULT, s)
+        if args.graph:
+            c.use_graph(True)
+        c.step(args.warmup)
+        if args.graph:
+            c.prepare_graph()
+        d0 = c.reduce()
+        c.step(args.fp64_loop_steps)
+        t = c.timings()
+        d1 = c.reduce()
+        pairs += d1["pairs_total"] - d0["pairs_total"]
+        tm = [a + x for a, x in zip(tm, t)]
+        c.close()
+    return passes * pairs / (tm[4] * 1e-3), tm, len(boxes), args.fp64_loop_steps
+
+
+def errors_after_one_step(args, rank, world):
+    """FP32-compensated step against the FP64-plain step from the same state."""
+    import spearhed_b200 as sb
+    from spearhed_b200 import abi
+    wa = make_workload(args, abi.PREC_FP32_COMP, rank, world)
+    ca = sb.context_for(wa)
+    ca.step(1)
+    ga = ca.get_species(0)
+    ca.close()
+    wb = make_workload(args, abi.PREC_FP64, rank, world)
+    cb = sb.context_for(wb)
+    cb.step(1)
+    gb = cb.get_species(0)
+    cb.close()
+    err_rho = float(np.max(np.abs(ga.density / gb.density - 1.0)))
+    err_acc = float(np.max(np.abs(ga.dvdt - gb.dvdt)) / np.max(np.abs(gb.dvdt)))
+    dBmax = float(np.max(np.abs(gb.dBdt)))
+    err_dB = float(np.max(np.abs(ga.dBdt - gb.dBdt)) / dBmax) if dBmax > 0 else None
+    return {"density_rel_max": err_rho, "accel_normwise": err_acc, "dBdt_normwise": err_dB,
+            "bounds": {"density_rel_max": 1e-5, "accel_normwise": 1e-4}}
+
+
+def e2e_leg(args, rank, world, tune, L):
+    """The metric through the C ABI with pinned host buffers: set, step, get."""
+    import torch
+
+    import spearhed_b200 as sb
+    from spearhed_b200 import abi
+    wi = make_workload(args, abi.PREC_FP32_COMP, rank, world)
+    n = wi.n
+    cols_in = ["pos", "vel", "mass", "h", "density", "u", "B", "psi"]
+    cols_out = ["pos", "vel", "density", "u", "B", "psi"]
+    # one set of pinned host columns: each step sends them and reads the
+    # step's result back into the same arrays
+    host = pinned_species(wi.species[0], cols_in)
+    params, boxes = wi.params, wi.boxes
+    del wi
+    params.device = int(os.environ.get("LOCAL_RANK", 0))
+    ce = sb.Context(params, boxes)
+    ce.set_species(0, host)
+    ce.set_tuning(tune["density_variant"], tune["force_variant"])
+    ce.step(1)
+    ce.get_species(0)  # allocations + list sizing happen here, outside timing
+    vin, vout = host.view(), host.view()
+    for f in ("dvdt", "dudt", "dBdt", "dpsidt", "divB"):
+        if f in abi.VECTOR_COLUMNS:
+            for a in range(3):
+                getattr(vin, f)[a] = None
+                getattr(vout, f)[a] = None
+        else:
+            setattr(vin, f, None)
+            setattr(vout, f, None)
+    for f in ("mass", "h"):
+        setattr(vout, f, None)
+    vin.box_id = None
+    vout.box_id = None
+    pe0 = ce.reduce()["pairs_total"]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        abi.check(L.sph_set_species(ce._p, 0, abi.ROLES_DEFAULT, host.n, C.byref(vin)))
+        abi.check(L.sph_step(ce._p, 1, 0.0))
+        abi.check(L.sph_get_species(ce._p, 0, C.byref(vout)))
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    pe1 = ce.reduce()["pairs_total"]
+    ce.close()
+    e2e_pairs = (pe1 - pe0) / args.e2e_steps
+    h2d = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_in) * 8 * n
+    d2h = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_out) * 8 * n
+    return e2e_pairs, e2e_s, h2d, d2h
+
+
+def reference_physics_leg(args, dev):
+    """The 512 boxes under the reference's own step, FP32 on the GPU."""
+    from spearhed_b200 import abi, setups
+    w = setups.brio_wu_ensemble(precision=abi.PREC_FP32_COMP, reference_physics=True)
+    ctx, shapes = prepared_context(w, dev, args)
+    r = timed_steps(ctx, args.steps, dev)
+    ctx.close()
+    passes = 2
+    return {"value": passes * r["pairs"] / (r["ms"] * 1e-3), "unit": UNIT, "ms_per_step": r["ms"] / args.steps,
+            "pairs_per_pass_per_step": r["pairs"] / args.steps, "pair_passes_per_step": passes,
+            "particles": w.n, "boxes": len(w.boxes), "stage_ms_per_step": stage_dict(r["stages"], args.steps),
+            "physics": "the reference's: density + inviscid hydro (P dV), cubic spline, one constant h per box "
+                       "(1.2 left spacings), radius 2h, constant dt, no periodic images; FP32 compensated"}
+
+
+def orszag_tang_leg(args, dev, peak):
+    """The Orszag-Tang slab (1,048,576 particles), FP32 and FP64: extra key."""
+    from spearhed_b200 import abi, flops, setups
+    out = {}
+    for prec, steps in ((abi.PREC_FP32_COMP, args.steps), (abi.PREC_FP64, args.fp64_steps)):
+        w = setups.orszag_tang(precision=prec)
+        ctx, _ = prepared_context(w, dev, args)
+        r = timed_steps(ctx, steps, dev)
+        ctx.close()
+        key = "fp32" if prec == abi.PREC_FP32_COMP else "fp64"
+        out[key] = {"value": 3 * r["pairs"] / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / steps,
+                    "stage_ms_per_step": stage_dict(r["stages"], steps)}
+        if key == "fp32":
+            ps = r["pairs"] / steps
+            d_ms, f_ms = r["stages"][1] / steps, r["stages"][2] / steps
+            out["fp32"]["density_frac"] = flops.DENSITY_FLOPS["wendland_c2"] * ps / (d_ms * 1e-3) / 1e12 / peak
+            out["fp32"]["force_frac"] = flops.FORCE_FLOPS["mhd"] * ps / (f_ms * 1e-3) / 1e12 / peak
+            out["particles"] = w.n
+    out["fp32_speedup"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["unit"] = UNIT
+    out["workload"] = "orszag_tang_slab_512x512x4"
+    return out
+
+
 # ------------------------------------------------------------------ main
 def run_ours(args, rank, world):
     import torch
 
-    import spearhed_b200 as sb
-    from spearhed_b200 import abi, flops, setups
+    from spearhed_b200 import abi, flops
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -334,39 +604,25 @@ def run_ours(args, rank, world):
     L.sphx_launch_count.restype = C.c_ulonglong
 
     wl_name, wl_kernel, wl_phys = WORKLOADS[args.workload]
+    ensemble = args.workload == "brio_wu_ensemble"
     # ensembles shard their boxes over the ranks; a single box runs one replica per rank
-    sharded = args.workload == "brio_wu_ensemble" and world > 1
+    sharded = ensemble and world > 1
     w = make_workload(args, abi.PREC_FP32_COMP, rank, world)
-    w.params.device = dev
     n = w.n
-    ctx = sb.context_for(w)
-    if args.graph:
-        ctx.use_graph(True)
-    ctx.step(args.warmup)
-    # launch shapes picked on this workload, before the timed region
-    tune = ctx.tuning() if args.no_tune else ctx.autotune(2)
-    if args.graph:
-        warm_graphs(ctx)
-    torch.cuda.synchronize()
+    nbox = len(w.boxes)
+    global_boxes = w.meta.get("global_boxes", [0])
+    adaptive = bool(w.params.physics & abi.PHYS_ADAPTIVE_H)
+    ctx, tune = prepared_context(w, dev, args)
+    del w
 
     def barrier():
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
 
-    d0 = ctx.reduce()
-    barrier()
-    torch.cuda.synchronize()
-    launches0 = L.sphx_launch_count()
-    with ClockSampler(dev) as clk:
-        ctx.step(args.steps)
-        torch.cuda.synchronize()
-    launches = L.sphx_launch_count() - launches0
-    barrier()
-    tm = ctx.timings()  # [build, density, force, kick, whole] ms over the timed steps
-    d1 = ctx.reduce()
-    pairs = d1["pairs_total"] - d0["pairs_total"]
-    ms_total = tm[4]
+    r = timed_steps(ctx, args.steps, dev, L=L, barrier=barrier, clocks=True)
+    ctx.close()
+    ms_total, pairs = r["ms"], r["pairs"]
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([ms_total, pairs], dtype=torch.float64, device=f"cuda:{dev}")
@@ -377,16 +633,17 @@ def run_ours(args, rank, world):
     passes = flops.PASSES_PER_STEP[wl_phys]
     value = passes * pairs / (ms_total * 1e-3)
     ms_step = ms_total / args.steps
+    tm = r["stages"]
 
     def profiled(name):
         # DRAM bytes per launch from the committed capture, for its own configuration only
         return traffic_from_profiles(name) if profiled_config(args) else None
 
     # Roofline of the dominant kernel (the longer of the two pair kernels; both
-    # are FP32 FMA-pipe bound).  Algorithmic flops count accepted pairs only;
+    # are FP32-pipe / issue bound).  Algorithmic flops count accepted pairs only;
     # the density kernel's cull of rejected candidates is reported beside it.
-    pairs_step = pairs / args.steps / max(world, 1)
-    cand_step = d1["candidates"]
+    pairs_step = r["pairs"] / args.steps
+    cand_step = r["candidates"]
     force_ms = tm[2] / args.steps
     dens_ms = tm[1] / args.steps
     peak = C.c_double(0)
@@ -396,17 +653,16 @@ def run_ours(args, rank, world):
     if force_ms <= 0 or dens_ms <= 0:
         # every timed step, graph-replayed or not, records its stage events
         raise RuntimeError("no per-stage event times from the timed steps")
+    prof = PROFILED.get(args.workload, (f"density_fp32_{args.workload}.txt", f"force_{wl_phys}_fp32_{args.workload}.txt"))
     force_achieved = flops.FORCE_FLOPS[wl_phys] * pairs_step / (force_ms * 1e-3) / 1e12
     dens_achieved = flops.DENSITY_FLOPS[wl_kernel] * pairs_step / (dens_ms * 1e-3) / 1e12
     cull_achieved = flops.CULL_FLOPS_PER_CANDIDATE * cand_step / (dens_ms * 1e-3) / 1e12
     force_info = {"kernel": f"kForce<{wl_kernel},float,{wl_phys}>", "ms_per_launch": force_ms,
                   "achieved": force_achieved, "frac": force_achieved / peak.value if peak.value else None,
-                  "flops_per_pair": flops.FORCE_FLOPS[wl_phys],
-                  "traffic": profiled(f"force_{wl_phys}_fp32_{args.workload}.txt")}
+                  "flops_per_pair": flops.FORCE_FLOPS[wl_phys], "traffic": profiled(prof[1])}
     dens_info = {"kernel": f"kDensity<{wl_kernel},float>", "ms_per_launch": dens_ms,
                  "achieved": dens_achieved, "frac": dens_achieved / peak.value if peak.value else None,
-                 "flops_per_pair": flops.DENSITY_FLOPS[wl_kernel],
-                 "traffic": profiled(f"density_fp32_{args.workload}.txt"),
+                 "flops_per_pair": flops.DENSITY_FLOPS[wl_kernel], "traffic": profiled(prof[0]),
                  "cull": {"candidates_per_launch": cand_step,
                           "efficiency": pairs_step / cand_step if cand_step else None,
                           "flops_per_candidate": flops.CULL_FLOPS_PER_CANDIDATE,
@@ -414,183 +670,125 @@ def run_ours(args, rank, world):
                           "frac_with_cull": (dens_achieved + cull_achieved) / peak.value if peak.value else None}}
     dominant, other = (dens_info, force_info) if dens_ms >= force_ms else (force_info, dens_info)
     result = {}
-    if rank == 0:
-        # ---- FP64 plain, same workload, same GPU
-        ctx.close()
-        if args.workload == "brio_wu_ensemble":
-            # the baseline of the ensemble: the FP64 single-box step looped over boxes
-            v64, t64 = fp64_box_loop(args, dev, passes)
-        else:
-            w64 = make_workload(args, abi.PREC_FP64, rank, world)
-            w64.params.device = dev
-            ctx64 = sb.context_for(w64)
-            if args.graph:
-                ctx64.use_graph(True)
-            ctx64.step(args.warmup)
-            if not args.no_tune:
-                ctx64.autotune(2)
-            if args.graph:
-                warm_graphs(ctx64)
-            e0 = ctx64.reduce()
-            ctx64.step(args.fp64_steps)
-            t64 = ctx64.timings()
-            e1 = ctx64.reduce()
-            v64 = passes * (e1["pairs_total"] - e0["pairs_total"]) / (t64[4] * 1e-3)
-            ctx64.close()
-        # ---- errors of the FP32 step against the FP64 step from the same state
-        wa = make_workload(args, abi.PREC_FP32_COMP, rank, world)
-        wb = make_workload(args, abi.PREC_FP64, rank, world)
-        ca, cb = sb.context_for(wa), sb.context_for(wb)
-        ca.step(1)
-        cb.step(1)
-        ga, gb = ca.get_species(0), cb.get_species(0)
-        err_rho = float(np.max(np.abs(ga.density / gb.density - 1.0)))
-        err_acc = float(np.max(np.abs(ga.dvdt - gb.dvdt)) / np.max(np.abs(gb.dvdt)))
-        dBmax = float(np.max(np.abs(gb.dBdt)))
-        err_dB = float(np.max(np.abs(ga.dBdt - gb.dBdt)) / dBmax) if dBmax > 0 else None
-        ca.close()
-        cb.close()
-        # ---- end to end through the C ABI with pinned host buffers
-        wi = make_workload(args, abi.PREC_FP32_COMP, rank, world)
-        cols_in = ["pos", "vel", "mass", "h", "density", "u", "B", "psi"]
-        cols_out = ["pos", "vel", "density", "u", "B", "psi"]
-        # one set of pinned host columns: each step sends them and reads the
-        # step's result back into the same arrays
-        host = pinned_species(wi.species[0], cols_in)
-        ce = sb.Context(wi.params, wi.boxes)
-        ce.set_species(0, host)
-        ce.set_tuning(tune["density_variant"], tune["force_variant"])
-        ce.step(1)
-        ce.get_species(0)  # allocations + list sizing happen here, outside timing
-        vin, vout = host.view(), host.view()
-        for f in ("dvdt", "dudt", "dBdt", "dpsidt", "divB"):
-            if f in abi.VECTOR_COLUMNS:
-                for a in range(3):
-                    getattr(vin, f)[a] = None
-                    getattr(vout, f)[a] = None
-            else:
-                setattr(vin, f, None)
-                setattr(vout, f, None)
-        for f in ("mass", "h"):
-            setattr(vout, f, None)
-        vin.box_id = None
-        vout.box_id = None
-        pe0 = ce.reduce()["pairs_total"]
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            abi.check(L.sph_set_species(ce._p, 0, abi.ROLES_DEFAULT, host.n, C.byref(vin)))
-            abi.check(L.sph_step(ce._p, 1, 0.0))
-            abi.check(L.sph_get_species(ce._p, 0, C.byref(vout)))
-        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-        pe1 = ce.reduce()["pairs_total"]
-        ce.close()
-        e2e_pairs = (pe1 - pe0) / args.e2e_steps
-        h2d = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_in) * 8 * n
-        d2h = sum((3 if f in abi.VECTOR_COLUMNS else 1) for f in cols_out) * 8 * n
-        # ---- CPU baseline (rank 0, N = 1 only)
-        cpu = None
-        if world == 1 and not args.no_cpu and args.workload == "orszag_tang":
-            cpu = cpu_reference_sample(args.nx, args.nz)
-        result = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
-            "dtype": "fp32 pair kernels (compensated), fp64 integration",
-            "data": "synthetic Orszag-Tang initial conditions (lattice, analytic v and B)",
-            "config": {"workload": wl_name if args.workload != "orszag_tang" or args.nx == 512 else
-                       f"orszag_tang_slab_{args.nx}x{args.nx}x{args.nz}", "particles": n, "kernel": wl_kernel,
-                       "boxes": len(w.boxes), "neighbours_mean": pairs_step / n,
-                       "physics": {"mhd": "hydro+AV+SPMHD+Dedner+CFL", "hydro_av": "hydro+AV+CFL"}[wl_phys]
-                       + ("+adaptive_h" if w.params.physics & abi.PHYS_ADAPTIVE_H else ""),
-                       "pair_passes_per_step": passes,
-                       "parallelism": (f"box_shards{world}" if sharded else f"replicas{world}") if world > 1 else "single",
-                       "l2": "working set > L2 (lists ~" + f"{n * 4 * 136 / 1e9:.2f}" + " GB, state ~0.3 GB)",
-                       "graph": bool(args.graph),
-                       "launch_shapes": {k: tune[k] for k in ("staging_depth", "density_blocks_per_sm",
-                                                              "force_blocks_per_sm", "steps_per_trial",
-                                                              "density_ms", "force_ms")}},
-            "stage_ms_per_step": {"sort_permute": tm[0] / args.steps, "density": dens_ms, "force": force_ms,
-                                  "kick_reduce": tm[3] / args.steps},
-            "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": t64[4] / args.fp64_steps,
-                           # per GPU: the FP64 leg runs on rank 0 alone
-                           "fp32_speedup": value / world / v64 if v64 else None,
-                           "stage_ms_per_step": {"sort_permute": t64[0] / args.fp64_steps,
-                                                 "density": t64[1] / args.fp64_steps,
-                                                 "force": t64[2] / args.fp64_steps,
-                                                 "kick_reduce": t64[3] / args.fp64_steps}},
-            "error_vs_fp64_after_1_step": {"density_rel_max": err_rho, "accel_normwise": err_acc,
-                                           "dBdt_normwise": err_dB},
-            "roofline": {"bound": "fp32_fma", **dominant, "peak": peak.value, "unit": "TFLOP/s",
-                         "pairs_per_launch": pairs_step,
-                         "peak_source": "measured live (FMA-chain microbenchmark, sphx_fma_tflops)",
-                         "other_pair_kernel": other,
-                         "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs"),
-                         # the same launch against HBM: ncu DRAM bytes per launch (profiles/)
-                         # over the event-timed launch, of the measured copy bandwidth
-                         "hbm": hbm_view(dominant, measured_peak("hbm_gbs"))},
-            "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
-            "gpu_launches": int(launches),
-            # step calls re-run after a neighbour-list overflow inside the timed region
-            # (a replay's first attempt is in the time, not in the pair count)
-            "list_replays_timed": int(d1["replays"] - d0["replays"]),
-            "clocks": clk.summary(),
-        }
-        if cpu is not None:
-            result["cpu_baseline"] = cpu
+    if rank != 0:
+        return result
+    # ---- FP64 plain on the same GPU: the batched context, and (ensemble) the single-box loop
+    w64 = make_workload(args, abi.PREC_FP64, rank, world)
+    c64, _ = prepared_context(w64, dev, args)
+    del w64
+    r64 = timed_steps(c64, args.fp64_steps, dev)
+    c64.close()
+    v64 = passes * r64["pairs"] / (r64["ms"] * 1e-3)
+    fp64 = {"batched": {"value": v64, "unit": UNIT, "ms_per_step": r64["ms"] / args.fp64_steps,
+                        "stage_ms_per_step": stage_dict(r64["stages"], args.fp64_steps),
+                        "fp32_speedup": value / world / v64 if v64 else None}}
+    if ensemble:
+        vl, tl, nb_loop, st_loop = fp64_box_loop(args, dev, passes, global_boxes)
+        fp64["box_loop"] = {"value": vl, "unit": UNIT, "boxes": nb_loop, "steps_per_box": st_loop,
+                            "ms_per_step_all_boxes": tl[4] / st_loop * (len(global_boxes) / nb_loop),
+                            "fp32_speedup": value / world / vl if vl else None,
+                            "what": "the FP64-plain single-box step looped over the boxes, one context per box; "
+                                    "device time summed over the boxes"}
+    fp64["value"] = fp64.get("box_loop", fp64["batched"])["value"]
+    fp64["fp32_speedup"] = fp64.get("box_loop", fp64["batched"])["fp32_speedup"]
+    # ---- errors of the FP32 step against the FP64 step from the same state
+    errs = errors_after_one_step(args, rank, world)
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e_pairs, e2e_s, h2d, d2h = e2e_leg(args, rank, world, tune, L)
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        if ensemble:
+            cpu = reference_box_sample(limit_s=args.cpu_seconds)
+        elif args.workload == "orszag_tang":
+            cpu = cpu_reference_sample(args.nx, args.nz, limit_s=args.cpu_seconds)
+    extra = {}
+    if ensemble and not args.no_extra:
+        extra["reference_physics"] = reference_physics_leg(args, dev)
+        if cpu is not None and cpu.get("value"):
+            extra["reference_physics"]["vs_cpu_reference"] = extra["reference_physics"]["value"] / cpu["value"]
+        extra["orszag_tang"] = orszag_tang_leg(args, dev, peak.value)
+    l2_note = "working set > L2 (state, records and neighbour lists of all boxes, several GB)"
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+        "dtype": "fp32 pair kernels (compensated), fp64 integration",
+        "data": "synthetic " + {"brio_wu_ensemble": "Brio-Wu shock-tube", "orszag_tang": "Orszag-Tang",
+                                "kelvin_helmholtz": "Kelvin-Helmholtz", "mhd_rotor": "MHD rotor",
+                                "sod_small": "Sod shock-tube"}[args.workload]
+                + " initial conditions (lattices, analytic fields, seeded jitter)",
+        "config": {"workload": wl_name if args.workload != "orszag_tang" or args.nx == 512 else
+                   f"orszag_tang_slab_{args.nx}x{args.nx}x{args.nz}", "particles": n, "kernel": wl_kernel,
+                   "boxes": nbox, "neighbours_mean": pairs_step / n,
+                   "physics": {"mhd": "hydro+AV+SPMHD+Dedner+CFL", "hydro_av": "hydro+AV+CFL"}[wl_phys]
+                   + ("+adaptive_h" if adaptive else ""),
+                   "pair_passes_per_step": passes,
+                   "parallelism": (f"box_shards{world}" if sharded else f"replicas{world}") if world > 1 else "single",
+                   "l2": l2_note, "graph": bool(args.graph),
+                   "launch_shapes": {k: tune[k] for k in ("staging_depth", "density_blocks_per_sm",
+                                                          "force_blocks_per_sm", "steps_per_trial",
+                                                          "density_ms", "force_ms")}},
+        "stage_ms_per_step": stage_dict(tm, args.steps),
+        "fp64_plain": fp64,
+        "error_vs_fp64_after_1_step": errs,
+        "roofline": {"bound": "fp32_fma", **dominant, "peak": peak.value, "unit": "TFLOP/s",
+                     "pairs_per_launch": pairs_step,
+                     "peak_source": "measured live (FMA-chain microbenchmark, sphx_fma_tflops)",
+                     "other_pair_kernel": other,
+                     "fp64_fma_peak": peak64.value, "hbm_peak_gbs": measured_peak("hbm_gbs"),
+                     # the same launch against HBM: ncu DRAM bytes per launch (profiles/)
+                     # over the event-timed launch, of the measured copy bandwidth
+                     "hbm": hbm_view(dominant, measured_peak("hbm_gbs"))},
+        "e2e": {"value": passes * e2e_pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": int(r["launches"]),
+        # step calls re-run after a neighbour-list overflow inside the timed region
+        # (a replay's first attempt is in the time, not in the pair count)
+        "list_replays_timed": r["replays"],
+        "clocks": r["clocks"],
+    }
+    if cpu is not None:
+        result["cpu_baseline"] = cpu
+    if ensemble:
+        result["arms"] = {
+            "same_config": False,
+            "differences": [
+                "value: the full north-star step (AV, SPMHD, Dedner, adaptive h, periodic images, 3 pair passes); "
+                "the reference has none of these, so the reference arm runs its own step on the same boxes",
+                "reference_physics: this GPU on exactly the reference arm's step and pair set (same 512 boxes, "
+                "density + inviscid hydro, one constant h per box, no periodic images, 2 pair passes)",
+                "the reference arm times a seeded random sample of whole boxes on the host cores; the GPU legs "
+                "time all 512 boxes",
+            ]}
+    result.update(extra)
     return result
 
 
-def fp64_box_loop(args, dev, passes):
-    """FP64 plain single-box contexts looped over a sample of the ensemble's
-    boxes (the largest and smallest first, then evenly spaced), each for
-    --fp64-steps after --warmup; returns (pair-interactions/s, summed timings)."""
-    import spearhed_b200 as sb
-    from spearhed_b200 import abi, setups
-    import numpy as np
-    # the ensemble's box sizes (same draw as setups.brio_wu_ensemble: Philox key 5)
-    ens_sizes = np.exp(np.random.Generator(np.random.Philox(key=5)).uniform(np.log(4096), np.log(262144), 512)).astype(int)
-    pick = np.linspace(0, len(ens_sizes) - 1, max(1, args.fp64_boxes)).astype(int)
-    pairs = 0.0
-    tm = [0.0] * 5
-    for b in pick:
-        p, box, s = setups.brio_wu_box(int(ens_sizes[b]), precision=abi.PREC_FP64)
-        p.device = dev
-        c = sb.Context(p, [box])
-        c.set_species(abi.SPECIES_DEFAULT, s)
-        if args.graph:
-            c.use_graph(True)
-        c.step(args.warmup)
-        if args.graph:
-            warm_graphs(c)
-        d0 = c.reduce()
-        c.step(args.fp64_steps)
-        t = c.timings()
-        d1 = c.reduce()
-        pairs += d1["pairs_total"] - d0["pairs_total"]
-        tm = [a + x for a, x in zip(tm, t)]
-        c.close()
-    return passes * pairs / (tm[4] * 1e-3), tm
-
-
-def main():
-    args = parse()
+def main(argv=None):
+    args = parse(argv)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cpu = cpu_reference_sample(args.nx, args.nz, limit_s=max(5.0, 2.0 * args.steps))
-        # the sample's time scaled to all target frames: one whole step of the
-        # reference's pair passes on this input (None for the oracle port)
-        fr = cpu.get("frames")
-        ms_step = cpu["seconds"] * 1e3 * fr[1] / fr[0] if fr and fr[0] and cpu.get("seconds") else None
+        limit = max(5.0, 2.0 * args.steps)
+        if args.workload == "brio_wu_ensemble":
+            cpu = reference_box_sample(limit_s=limit)
+            ms_step = None
+        else:
+            cpu = cpu_reference_sample(args.nx, args.nz, limit_s=limit)
+            # the sample's time scaled to all target frames: one whole step of the
+            # reference's pair passes on this input (None for the oracle port)
+            fr = cpu.get("frames")
+            ms_step = cpu["seconds"] * 1e3 * fr[1] / fr[0] if fr and fr[0] and cpu.get("seconds") else None
+        wl_name = WORKLOADS[args.workload][0] if args.workload in ("brio_wu_ensemble", "orszag_tang") else \
+            WORKLOADS["orszag_tang"][0]
         line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32" if cpu.get("kind") == "reference" else "fp64",
-                "data": "synthetic Orszag-Tang initial conditions",
-                "config": {"workload": "orszag_tang_slab_512x512x4"}, "impl": "reference",
+                "data": "synthetic initial conditions of the GPU arm's workload",
+                "config": {"workload": wl_name}, "impl": "reference",
                 "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                              "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)

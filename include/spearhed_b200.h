@@ -228,6 +228,22 @@ int sph_mhd(sph_ctx* ctx);
  * sph_reduce reports zero sums. */
 int sph_step(sph_ctx* ctx, int32_t n_steps, double dt);
 
+/* Bounded waits (no reference counterpart: its host waits are unbounded
+ * syncWait calls, include/spearhed/control/Simulation.x.cpp:303-307).  With a
+ * limit of `seconds` > 0, sph_step, sph_density, sph_hydro and sph_mhd wait at
+ * most that long for their device work (polling an event; 0, the default,
+ * waits without a limit).  When the limit passes the call returns
+ * SPH_ERR_TIMEOUT; its work keeps running and nothing is cancelled, and the
+ * call's checks (non-finite or escaped particles, list overflow) are still
+ * owed.  sph_wait completes them, and so does the next call on the context
+ * (every call that touches its device state, except sph_destroy, which waits
+ * without a limit); until then that next call returns SPH_ERR_TIMEOUT too.
+ * A completed call's results stand; a step call whose checks fail is rolled
+ * back to the state it started from and sph_wait returns the check's status
+ * (after a list overflow the lists have grown: run the call again). */
+int sph_set_wait_timeout(sph_ctx* ctx, double seconds);
+int sph_wait(sph_ctx* ctx);
+
 /* Conserved-quantity reductions of the current state (no reference counterpart;
  * PMacc's device::Reduce, packages/pmacc/include/pmacc/device/Reduce.hpp:41, is unused there). */
 int sph_reduce(sph_ctx* ctx, SphDiag* out);
@@ -382,6 +398,13 @@ int sph_density_noalloc(const SphParams* params, const SphBox* box, int64_t n, c
                         const double* z, const double* mass, const double* h, double* rho, void* stream);
 
 const char* sph_last_error_string(void);
+
+/* Test hook (no reference counterpart): the device allocation `after` places
+ * from now (0 = the next one) inside this library's contexts is refused with
+ * SPH_ERR_NOMEM, once; a negative value disarms it.  Used to check that every
+ * allocation point fails cleanly and leaves the context destroyable and
+ * usable again.  Returns the previous setting. */
+long long sphx_fail_alloc_after(long long after);
 
 #ifdef __cplusplus
 }

@@ -108,6 +108,14 @@ class Context:
         P = C.POINTER(C.c_double)
         abi.check(self._L.sph_set_clock(self._p, n, t.ctypes.data_as(P), d.ctypes.data_as(P)))
 
+    def set_wait_timeout(self, seconds: float):
+        """Bound the wait of the compute calls (0 = no limit); see sph_set_wait_timeout."""
+        abi.check(self._L.sph_set_wait_timeout(self._p, float(seconds)))
+
+    def wait(self):
+        """Complete a call that returned SPH_ERR_TIMEOUT (sph_wait)."""
+        abi.check(self._L.sph_wait(self._p))
+
     def use_graph(self, on: bool = True):
         abi.check(self._L.sph_use_graph(self._p, int(bool(on))))
 

@@ -285,6 +285,10 @@ def lib():
         "sph_set_tuning": (C.c_int, [ctx_p, C.c_int32, C.c_int32]),
         "sph_get_tuning": (C.c_int, [ctx_p, P(SphTuning)]),
         "sph_last_error_string": (C.c_char_p, []),
+        "sph_set_wait_timeout": (C.c_int, [ctx_p, C.c_double]),
+        "sph_wait": (C.c_int, [ctx_p]),
+        "sph_density_noalloc": (C.c_int, [P(SphParams), P(SphBox), C.c_int64] + [C.c_void_p] * 7),
+        "sphx_fail_alloc_after": (C.c_longlong, [C.c_longlong]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

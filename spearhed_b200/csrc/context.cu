@@ -13,12 +13,17 @@
 // asynchronous) into a staging column and gathered into the sorted state.
 #include "sph_launch.hpp"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace
@@ -145,6 +150,39 @@ namespace
 
 namespace sph
 {
+    //! NVTX range over a host scope (the launches of one pass, or one public
+    //! call): profilers show the passes by name; without a tool attached a
+    //! push/pop costs a branch.
+    struct NvtxRange
+    {
+        explicit NvtxRange(char const* name)
+        {
+            nvtxRangePushA(name);
+        }
+        ~NvtxRange()
+        {
+            nvtxRangePop();
+        }
+        NvtxRange(NvtxRange const&) = delete;
+        NvtxRange& operator=(NvtxRange const&) = delete;
+    };
+
+    //! Test hook (sphx_fail_alloc_after): device allocations left before the
+    //! next one is refused with SPH_ERR_NOMEM; negative = no injection.
+    std::atomic<long long> g_allocFailAfter{-1};
+
+    //! True when the injection hook refuses this allocation (it then disarms).
+    bool allocRefused()
+    {
+        long long k = g_allocFailAfter.load();
+        while(k >= 0)
+        {
+            if(g_allocFailAfter.compare_exchange_weak(k, k - 1))
+                return k == 0;
+        }
+        return false;
+    }
+
     //! Records the message sph_last_error_string() returns on this thread.
     int recordError(int code, std::string msg)
     {
@@ -206,6 +244,21 @@ struct sph_ctx
     }
     bool anyTwoLevel = false;                 //!< some box allocates level-1 cells
     uint32_t lastStat[sph::kStatWords] = {};  //!< status words of the last checkStatus
+    // Bounded waits (sph_set_wait_timeout): a compute call whose device work
+    // has not finished within waitLimit seconds returns SPH_ERR_TIMEOUT and
+    // leaves its checks pending; sph_wait or the next call completes them.
+    double waitLimit = 0.0;  //!< 0: wait without a limit
+    bool boundedWait = false; //!< the running public call honours waitLimit
+    cudaEvent_t eWait = nullptr;
+    enum Pending
+    {
+        kPendNone = 0,
+        kPendStep,
+        kPendDensity,
+        kPendForce
+    };
+    int pending = kPendNone;
+    int32_t pendingSteps = 0;
     SphTuning tuning{};
     bool haveSnap = false;
     sph::Master snap{};
@@ -223,6 +276,8 @@ struct sph_ctx
                     cudaEventDestroy(e);
         if(eCall)
             cudaEventDestroy(eCall);
+        if(eWait)
+            cudaEventDestroy(eWait);
         if(eCopy)
             cudaEventDestroy(eCopy);
         if(eCompute)
@@ -291,6 +346,8 @@ struct sph_ctx
         if(count == 0)
             count = 1;
         void* ptr = nullptr;
+        if(sph::allocRefused())
+            return fail(SPH_ERR_NOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes: refused (injected)");
         cudaError_t const e = cudaMalloc(&ptr, count * sizeof(T));
         if(e != cudaSuccess)
             return fail(
@@ -402,7 +459,11 @@ struct sph_ctx
     int growLists(uint32_t need, bool bestEffort = false);
     int build(bool drift);
     int clearStatus();
+    int waitStream(char const* where);
+    int evalStatus(char const* where);
     int checkStatus(char const* where);
+    int completePending();
+    void collectTimings(int32_t nsteps);
     int snapshot(bool restore);
     int runSteps(int32_t nsteps);
     int autotune(int32_t stepsPerTrial);
@@ -805,6 +866,7 @@ int sph_ctx::ensureDevice()
 //! Drift (optional) + cell keys + sort + cell ranges + permute/pack.
 int sph_ctx::build(bool drift)
 {
+    sph::NvtxRange const range(drift ? "drift + cell sort" : "cell sort");
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->pairs, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(&dc.scal->candidates, 0, sizeof(unsigned long long), stream));
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.chBits, 0, sizeof(unsigned long long) * dc.nbox, stream));
@@ -825,6 +887,7 @@ int sph_ctx::build(bool drift)
 
 int sph_ctx::densityPass()
 {
+    sph::NvtxRange const range("density pass");
     SPH_CUDA_TRY(cudaMemsetAsync(dc.lists.count, 0xff, size_t(n) * 4, stream));
     sph::launchDensity(dc, pa, p.kernel, p.precision, false, densityVariant, stream);
     return SPH_OK;
@@ -832,6 +895,7 @@ int sph_ctx::densityPass()
 
 int sph_ctx::forcePass()
 {
+    sph::NvtxRange const range("force pass");
     SPH_CUDA_TRY(cudaMemsetAsync(dc.bs.dtBits, 0x7f, sizeof(unsigned long long) * dc.nbox, stream));
     sph::launchForce(dc, pa, p.kernel, p.precision, forceVariant, stream);
     return SPH_OK;
@@ -883,12 +947,65 @@ int sph_ctx::snapshot(bool restore)
     return SPH_OK;
 }
 
+//! Waits for everything queued on the context's stream.  Inside a public call
+//! that honours the limit (sph_step, sph_density, sph_hydro, sph_mhd, sph_wait
+//! and the completion of a pending call), the wait polls an event against the
+//! deadline instead of blocking, and returns SPH_ERR_TIMEOUT when it passes
+//! (the work keeps running; nothing is cancelled).
+int sph_ctx::waitStream(char const* where)
+{
+    if(!boundedWait || !(waitLimit > 0.0))
+    {
+        SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+        return SPH_OK;
+    }
+    if(!eWait)
+        SPH_CUDA_TRY(cudaEventCreateWithFlags(&eWait, cudaEventDisableTiming));
+    SPH_CUDA_TRY(cudaEventRecord(eWait, stream));
+    auto const t0 = std::chrono::steady_clock::now();
+    std::chrono::microseconds nap(10);
+    for(;;)
+    {
+        cudaError_t const q = cudaEventQuery(eWait);
+        if(q == cudaSuccess)
+        {
+            // a "not ready" answer of the poll is not an error of this call
+            if(cudaPeekAtLastError() == cudaErrorNotReady)
+                cudaGetLastError();
+            return SPH_OK;
+        }
+        if(q != cudaErrorNotReady)
+            return fail(SPH_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(q));
+        double const el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if(el >= waitLimit)
+        {
+            if(cudaPeekAtLastError() == cudaErrorNotReady)
+                cudaGetLastError();
+            return fail(
+                SPH_ERR_TIMEOUT,
+                std::string(where) + ": the device work did not finish within " + std::to_string(waitLimit)
+                    + " s; it keeps running, and sph_wait (or the next call on this context) completes the call");
+        }
+        std::this_thread::sleep_for(nap);
+        nap = std::min(nap * 2, std::chrono::microseconds(1000));
+    }
+}
+
 int sph_ctx::checkStatus(char const* where)
 {
-    uint32_t* const stat = lastStat;
-    SPH_CUDA_TRY(cudaMemcpyAsync(stat, dc.status, sizeof(lastStat), cudaMemcpyDeviceToHost, stream));
+    int const w = waitStream(where);
+    if(w)
+        return w;
+    SPH_CUDA_TRY(cudaMemcpyAsync(lastStat, dc.status, sizeof(lastStat), cudaMemcpyDeviceToHost, stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
     SPH_CUDA_TRY(cudaGetLastError());
+    return evalStatus(where);
+}
+
+//! The status words of lastStat as a status code (and error message).
+int sph_ctx::evalStatus(char const* where)
+{
+    uint32_t const* const stat = lastStat;
     if(stat[sph::kStatNonFinite])
         return fail(
             SPH_ERR_NONFINITE,
@@ -930,7 +1047,10 @@ int sph_ctx::stepOnce(cudaEvent_t const* ev, bool capture)
         return st;
     if(ev)
         SPH_CUDA_TRY(recordStage(ev[3], capture));
-    sph::launchKick(dc, pa, (p.physics & SPH_PHYS_CFL) != 0, stream);
+    {
+        sph::NvtxRange const range("kick + reductions");
+        sph::launchKick(dc, pa, (p.physics & SPH_PHYS_CFL) != 0, stream);
+    }
     if(ev)
         SPH_CUDA_TRY(recordStage(ev[4], capture));
     return SPH_OK;
@@ -958,6 +1078,13 @@ int sph_ctx::steps(int32_t nsteps, double dt)
     for(int attempt = 0;; ++attempt)
     {
         st = runSteps(nsteps);
+        if(st == SPH_ERR_TIMEOUT)
+        {
+            pending = kPendStep;
+            pendingSteps = nsteps;
+            densityValid = forceValid = false;
+            return st;
+        }
         if(st == SPH_ERR_OVERFLOW && attempt == kMaxReplays)
         {
             // give up with the state the call started from
@@ -1216,8 +1343,18 @@ int sph_ctx::runSteps(int32_t nsteps)
             return st;
     SPH_CUDA_TRY(cudaEventRecord(eEnd, stream));
     st = checkStatus("sph_step");
+    if(st != SPH_ERR_TIMEOUT)
+        collectTimings(nsteps);
+    return st;
+}
+
+//! Per-stage and whole-run times of the last runSteps (its events have completed).
+void sph_ctx::collectTimings(int32_t nsteps)
+{
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, eBeg, eEnd);
+    for(double& t : timings)
+        t = 0.0;
+    cudaEventElapsedTime(&ms, events[0], events[1]);
     timings[4] = ms;
     for(int32_t s = 0; s < nsteps; ++s)
         for(int k = 0; k < 4; ++k)
@@ -1225,6 +1362,61 @@ int sph_ctx::runSteps(int32_t nsteps)
             cudaEventElapsedTime(&ms, events[2 + size_t(s) * 5 + k], events[2 + size_t(s) * 5 + k + 1]);
             timings[k] += ms;
         }
+}
+
+//! Completes a call that returned SPH_ERR_TIMEOUT: waits (bounded) for its
+//! work, then runs the checks it skipped.  A step call whose checks fail is
+//! rolled back to the state it started from (its lists grown after an
+//! overflow) and returns their status; a density call that overflowed grows
+//! the lists.  Returns SPH_ERR_TIMEOUT while the work is still running.
+int sph_ctx::completePending()
+{
+    if(pending == kPendNone)
+        return SPH_OK;
+    SPH_CUDA_TRY(cudaSetDevice(p.device));
+    bool const bw = boundedWait;
+    boundedWait = true;
+    char const* const where = pending == kPendStep ? "sph_step" : (pending == kPendDensity ? "sph_density" : "sph_hydro");
+    int st = checkStatus(where);
+    boundedWait = bw;
+    if(st == SPH_ERR_TIMEOUT)
+        return st;
+    int const kind = pending;
+    pending = kPendNone;
+    if(st == SPH_ERR_OVERFLOW && kind != kPendForce)
+    {
+        int const g = growLists(uint32_t(double(lastStat[sph::kStatOverflow]) * 1.25) + 16);
+        if(g)
+            return g;
+        st = fail(SPH_ERR_OVERFLOW,
+                  std::string(where) + ": a neighbour list overflowed; the lists have grown, run the call again");
+    }
+    if(kind == kPendStep)
+    {
+        if(st == SPH_OK)
+        {
+            collectTimings(pendingSteps);
+            float ms = 0.f;
+            if(eCall && cudaEventElapsedTime(&ms, eCall, events[1]) == cudaSuccess)
+                timings[4] = ms;
+            densityValid = forceValid = true;
+            return SPH_OK;
+        }
+        // the call's checks failed: back to the state it started from
+        int const rs = snapshot(true);
+        if(rs)
+            return rs;
+        SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+        densityValid = forceValid = false;
+        return st;
+    }
+    if(kind == kPendDensity)
+    {
+        densityValid = st == SPH_OK;
+        forceValid = false;
+        return st;
+    }
+    forceValid = st == SPH_OK;
     return st;
 }
 
@@ -1307,6 +1499,8 @@ namespace
         cudaError_t take(T*& out, size_t count)
         {
             void* p = nullptr;
+            if(sph::allocRefused())
+                return cudaErrorMemoryAllocation;
             cudaError_t const e = cudaMalloc(&p, (count ? count : 1) * sizeof(T));
             if(e == cudaSuccess)
                 ptrs.push_back(p);
@@ -1315,6 +1509,33 @@ namespace
         }
     };
 } // namespace
+
+namespace
+{
+    //! Marks a public compute call whose waits honour the context's limit.
+    struct BoundedCall
+    {
+        sph_ctx* c;
+        explicit BoundedCall(sph_ctx* ctx) : c(ctx)
+        {
+            c->boundedWait = true;
+        }
+        ~BoundedCall()
+        {
+            c->boundedWait = false;
+        }
+    };
+} // namespace
+
+//! Every public call that touches a context's device state first completes a
+//! call of that context that returned SPH_ERR_TIMEOUT (see sph_wait).
+#define SPH_COMPLETE_PENDING(ctx)                                                                                      \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        int const pst_ = (ctx)->completePending();                                                                     \
+        if(pst_)                                                                                                       \
+            return pst_;                                                                                               \
+    } while(0)
 
 extern "C" {
 
@@ -1378,6 +1599,7 @@ int sph_set_boxes(sph_ctx* ctx, int32_t nbox, SphBox const* boxes)
 {
     if(!ctx || nbox < 1 || !boxes)
         return fail(SPH_ERR_INVALID, "sph_set_boxes: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     for(int32_t b = 0; b < nbox; ++b)
         for(int a = 0; a < 3; ++a)
             if(!(boxes[b].hi[a] > boxes[b].lo[a]) || !std::isfinite(boxes[b].lo[a]) || !std::isfinite(boxes[b].hi[a]))
@@ -1398,6 +1620,7 @@ int sph_set_species(sph_ctx* ctx, int32_t species_id, uint32_t roles, int64_t n,
 {
     if(!ctx || species_id < 0 || species_id >= SPH_NUM_SPECIES || n < 0 || (n > 0 && !v))
         return fail(SPH_ERR_INVALID, "sph_set_species: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     if(n > 0 && (!v->pos[0] || !v->pos[1] || !v->pos[2]))
         return fail(SPH_ERR_INVALID, "sph_set_species: positions are required");
     if((roles & SPH_ROLE_SOURCE) && n > 0 && !v->mass)
@@ -1434,13 +1657,21 @@ int sph_density(sph_ctx* ctx)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    SPH_COMPLETE_PENDING(ctx);
     if(ctx->empty())
         return SPH_OK;
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    BoundedCall const bounded(ctx);
     int st = ctx->ensureDevice();
     if(st || (st = ctx->clearStatus()) || (st = ctx->build(false)) || (st = ctx->densityPass()))
         return st;
     st = ctx->checkStatus("sph_density");
+    if(st == SPH_ERR_TIMEOUT)
+    {
+        ctx->pending = sph_ctx::kPendDensity;
+        ctx->densityValid = ctx->forceValid = false;
+        return st;
+    }
     if(st == SPH_ERR_OVERFLOW)
     {
         uint32_t stat[sph::kStatWords];
@@ -1452,7 +1683,14 @@ int sph_density(sph_ctx* ctx)
         SPH_CUDA_TRY(cudaMemsetAsync(&ctx->dc.scal->candidates, 0, sizeof(unsigned long long), ctx->stream));
         SPH_CUDA_TRY(cudaMemsetAsync(ctx->dc.bs.chBits, 0, sizeof(unsigned long long) * ctx->dc.nbox, ctx->stream));
         if((st = ctx->densityPass()) || (st = ctx->checkStatus("sph_density")))
+        {
+            if(st == SPH_ERR_TIMEOUT)
+            {
+                ctx->pending = sph_ctx::kPendDensity;
+                ctx->densityValid = ctx->forceValid = false;
+            }
             return st;
+        }
     }
     else if(st)
         return st;
@@ -1465,14 +1703,23 @@ int sph_hydro(sph_ctx* ctx)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    SPH_COMPLETE_PENDING(ctx);
     if(ctx->empty())
         return SPH_OK;
     if(!ctx->densityValid)
         return fail(SPH_ERR_STATE, "sph_hydro needs the density of the current state (call sph_density first)");
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    BoundedCall const bounded(ctx);
     int st = ctx->forcePass();
     if(st || (st = ctx->checkStatus("sph_hydro")))
+    {
+        if(st == SPH_ERR_TIMEOUT)
+        {
+            ctx->pending = sph_ctx::kPendForce;
+            ctx->forceValid = false;
+        }
         return st;
+    }
     ctx->forceValid = true;
     return SPH_OK;
 }
@@ -1490,6 +1737,7 @@ int sph_step(sph_ctx* ctx, int32_t n_steps, double dt)
 {
     if(!ctx || n_steps < 0 || !std::isfinite(dt))
         return fail(SPH_ERR_INVALID, "sph_step: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     if(ctx->empty())
     {
         ctx->emptySteps += n_steps;
@@ -1497,13 +1745,36 @@ int sph_step(sph_ctx* ctx, int32_t n_steps, double dt)
         return SPH_OK;
     }
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    BoundedCall const bounded(ctx);
+    sph::NvtxRange const range("sph_step");
     return ctx->steps(n_steps, dt);
+}
+
+long long sphx_fail_alloc_after(long long after)
+{
+    return sph::g_allocFailAfter.exchange(after < 0 ? -1 : after);
+}
+
+int sph_set_wait_timeout(sph_ctx* ctx, double seconds)
+{
+    if(!ctx || !(seconds >= 0.0) || !std::isfinite(seconds))
+        return fail(SPH_ERR_INVALID, "sph_set_wait_timeout: bad arguments");
+    ctx->waitLimit = seconds;
+    return SPH_OK;
+}
+
+int sph_wait(sph_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SPH_ERR_INVALID, "null context");
+    return ctx->completePending();
 }
 
 int sph_get_species(sph_ctx* ctx, int32_t species_id, SphSoAView* v)
 {
     if(!ctx || !v || species_id < 0 || species_id >= SPH_NUM_SPECIES)
         return fail(SPH_ERR_INVALID, "sph_get_species: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     HostSpecies const& s = ctx->sp[species_id];
     if(s.declared && s.n == 0)
         return SPH_OK; // nothing to copy
@@ -1579,6 +1850,7 @@ int sph_get_neighbour_counts(sph_ctx* ctx, int32_t species_id, int32_t* counts)
 {
     if(!ctx || !counts || species_id < 0 || species_id >= SPH_NUM_SPECIES)
         return fail(SPH_ERR_INVALID, "sph_get_neighbour_counts: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     HostSpecies const& s = ctx->sp[species_id];
     if(s.declared && s.n == 0)
         return SPH_OK;
@@ -1654,6 +1926,7 @@ int sph_reduce(sph_ctx* ctx, SphDiag* out)
 {
     if(!ctx || !out)
         return fail(SPH_ERR_INVALID, "sph_reduce: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     if(ctx->empty())
     {
         *out = SphDiag{};
@@ -1693,6 +1966,7 @@ int sph_ensemble_reduce(sph_ctx* ctx, int32_t nbox, SphDiag* out)
 {
     if(!ctx || !out || nbox < 1)
         return fail(SPH_ERR_INVALID, "sph_ensemble_reduce: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     if(ctx->empty())
     {
         if(size_t(nbox) != std::max<size_t>(1, ctx->boxes.size()))
@@ -1729,6 +2003,7 @@ int sph_get_clock(sph_ctx* ctx, int32_t nbox, double* time, double* dt_next)
 {
     if(!ctx || nbox < 1 || !time || !dt_next)
         return fail(SPH_ERR_INVALID, "sph_get_clock: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     int st = ctx->ensureDevice();
     if(st)
@@ -1745,6 +2020,7 @@ int sph_set_clock(sph_ctx* ctx, int32_t nbox, double const* time, double const* 
 {
     if(!ctx || nbox < 1 || !time || !dt_next)
         return fail(SPH_ERR_INVALID, "sph_set_clock: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     for(int32_t b = 0; b < nbox; ++b)
         if(!std::isfinite(time[b]) || !(dt_next[b] > 0.0) || !std::isfinite(dt_next[b]))
             return fail(SPH_ERR_INVALID, "sph_set_clock: time must be finite and dt positive");
@@ -1781,6 +2057,7 @@ int sph_prepare_graph(sph_ctx* ctx)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    SPH_COMPLETE_PENDING(ctx);
     if(!ctx->useGraph || ctx->empty())
         return SPH_OK;
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
@@ -1799,6 +2076,7 @@ int sph_init_lattice(
 {
     if(!ctx || species_id < 0 || species_id >= SPH_NUM_SPECIES || nblocks < 0 || (nblocks > 0 && !blocks))
         return fail(SPH_ERR_INVALID, "sph_init_lattice: bad arguments");
+    SPH_COMPLETE_PENDING(ctx);
     SphInitProfile prof{};
     if(profile)
         prof = *profile;
@@ -1970,6 +2248,7 @@ int sph_autotune(sph_ctx* ctx, int32_t steps_per_trial, SphTuning* out)
 {
     if(!ctx)
         return fail(SPH_ERR_INVALID, "null context");
+    SPH_COMPLETE_PENDING(ctx);
     SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
     int const st = ctx->autotune(steps_per_trial);
     if(st)

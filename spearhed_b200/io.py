@@ -145,3 +145,77 @@ def resume(path):
         ctx.set_species(sid, s)
     ctx.set_clock(ck.time, ck.dt)
     return ctx, ck
+
+
+# ---------------------------------------------------------------- diagnostics
+DIAG_FORMAT = "spearhed_b200.diagnostics/1"
+
+
+class DiagnosticsLog:
+    """Per-step diagnostics as JSON lines (one object per record() call).
+
+    Each line holds the step count and simulated time, the dt of the last step
+    and the next one, the conserved quantities of sph_reduce (kinetic, internal,
+    magnetic and total energy, momentum, <|div B| h/|B|> and its maximum, the
+    Dedner speed), the accepted pairs of the last pass and the device time of
+    the last call per stage (sph_get_timings: sort+permute, density, force,
+    integrate+reduce, whole call).  The first line is a header with the format
+    name.  The reference logs progress to stdout only
+    (pmacc/simulationControl/SimulationHelper.cpp:89-108)."""
+
+    STAGES = ("sort_permute_ms", "density_ms", "force_ms", "kick_reduce_ms", "call_ms")
+
+    def __init__(self, path, meta=None):
+        self.path = path
+        self._f = open(path, "w")
+        self._f.write(json.dumps({"format": DIAG_FORMAT, **(meta or {})}) + "\n")
+        self._f.flush()
+
+    def record(self, ctx, extra=None):
+        d = ctx.reduce()
+        tm = ctx.timings()
+        row = {"step": int(d["steps"]), "time": d["time"], "dt": d["dt"], "dt_next": d["dt_next"],
+               "e_kin": d["e_kin"], "e_int": d["e_int"], "e_mag": d["e_mag"],
+               "e_tot": d["e_kin"] + d["e_int"] + d["e_mag"], "mom": list(d["mom"]),
+               "divb_mean": d["divb_mean"], "divb_max": d["divb_max"], "c_h": d["c_h"],
+               "pairs": d["pairs"], "replays": int(d["replays"])}
+        row.update({k: float(v) for k, v in zip(self.STAGES, tm)})
+        if extra:
+            row.update(extra)
+        self._f.write(json.dumps(row) + "\n")
+        self._f.flush()
+        return row
+
+    def close(self):
+        if self._f:
+            self._f.close()
+            self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def run_logged(ctx, n_steps, path, every=1, dt=0.0, meta=None):
+    """Steps `ctx` n_steps times, `every` steps per call, and logs one
+    diagnostics line per call to `path` (JSON lines).  Returns the rows."""
+    rows = []
+    with DiagnosticsLog(path, meta) as log:
+        done = 0
+        while done < n_steps:
+            k = min(every, n_steps - done)
+            ctx.step(k, dt)
+            done += k
+            rows.append(log.record(ctx))
+    return rows
+
+
+def read_diagnostics(path):
+    """(header, rows) of a diagnostics log."""
+    with open(path) as f:
+        lines = [json.loads(x) for x in f if x.strip()]
+    if not lines or lines[0].get("format") != DIAG_FORMAT:
+        raise ValueError(f"{path}: not a {DIAG_FORMAT} log")
+    return lines[0], lines[1:]

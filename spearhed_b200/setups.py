@@ -282,17 +282,28 @@ def orszag_tang(nx=512, nz=4, precision=abi.PREC_FP32_COMP, hfact=1.45, jitter=0
     return _workload("orszag_tang", params, [box], {abi.SPECIES_DEFAULT: init}, 200, {"nx": nx, "nz": nz, "dx": dx})
 
 
-def _brio_wu_blocks(n_target, precision, nt, box_id):
+def _brio_wu_blocks(n_target, precision, nt, box_id, reference_physics=False):
     gamma = 2.0
     nxl = max(8, int(round(n_target / (nt * nt * 1.125))))
     nxl += nxl % 2
     dxl = 0.5 / nxl
     L = nt * dxl
     m = dxl ** 3
+    # reference physics: one constant h per box (the reference's h0 is both the
+    # cull radius / 2 and every particle's h), here the left state's 1.2 dxl
+    hr = 1.2 * dxl if reference_physics else 2.4 * dxl
     left = LatticeBlock((-0.5, 0.0, 0.0), (0.0, L, L), counts=(nxl, nt, nt), box_id=box_id, mass=m, h=1.2 * dxl,
                         density=1.0, u=1.0 / ((gamma - 1.0) * 1.0), B=(0.75, 1.0, 0.0))
     right = LatticeBlock((0.0, 0.0, 0.0), (0.5, L, L), counts=(nxl // 2, nt // 2, nt // 2), box_id=box_id, mass=m,
-                         h=2.4 * dxl, density=0.125, u=0.1 / ((gamma - 1.0) * 0.125), B=(0.75, -1.0, 0.0))
+                         h=hr, density=0.125, u=0.1 / ((gamma - 1.0) * 0.125), B=(0.75, -1.0, 0.0))
+    if reference_physics:
+        # the reference's step: inviscid hydro, constant h and dt, no periodic
+        # images (its region search has none); the pair-max cull with one h per
+        # box is the reference's global radius 2 h0 box by box
+        params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
+                                    physics=0, gamma=gamma, h0=1.2 * dxl, dt=1e-5)
+        box = abi.make_box((-0.75, 0.0, 0.0), (0.75, L, L), (0, 0, 0))
+        return params, box, [left, right]
     physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
                | abi.PHYS_ADAPTIVE_H)
     params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
@@ -316,7 +327,15 @@ def brio_wu_box(n_target=8192, precision=abi.PREC_FP32_COMP, nt=8, box_id=0):
     return params, box, LatticeInit(blocks).generate()
 
 
-def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144, rank=0, world=1):
+def brio_wu_sizes(nbox=512, seed=5, n_lo=4096, n_hi=262144):
+    """Target particle counts of the ensemble's boxes: log-uniform in
+    [n_lo, n_hi] (numpy Philox, key ``seed``)."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    return np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=nbox)).astype(int)
+
+
+def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, n_hi=262144, rank=0, world=1,
+                     reference_physics=False, boxes=None):
     """An ensemble of independent Brio-Wu tubes with particle counts drawn
     log-uniform in [n_lo, n_hi] (numpy Philox, key ``seed``).  With the default
     512 boxes this is about 31 M particles.  Every box keeps its own time step.
@@ -325,22 +344,28 @@ def brio_wu_ensemble(nbox=512, precision=abi.PREC_FP32_COMP, seed=5, n_lo=4096, 
 
     With ``world`` > 1 only the boxes that longest-processing-time assigns to
     ``rank`` are built (renumbered from 0; their global ids are in
-    ``meta["global_boxes"]``), so each rank generates only its own particles."""
+    ``meta["global_boxes"]``), so each rank generates only its own particles.
+
+    ``reference_physics`` builds the same particles under the reference's own
+    step (inviscid hydro, one constant h per box, constant dt, no periodic
+    images); ``boxes`` (global ids) builds only those boxes."""
     from .ensemble import lpt_partition
-    rng = np.random.Generator(np.random.Philox(key=seed))
-    sizes = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=nbox)).astype(int)
+    sizes = brio_wu_sizes(nbox, seed, n_lo, n_hi)
     mine = np.arange(nbox) if world <= 1 else np.flatnonzero(lpt_partition(sizes, world) == rank)
-    boxes, blocks, params = [], [], None
+    if boxes is not None:
+        mine = np.asarray(boxes, dtype=np.int64)
+    blist, blocks, params = [], [], None
     for local, b in enumerate(mine):
-        p, box, bl = _brio_wu_blocks(int(sizes[b]), precision, 8, local)
-        boxes.append(box)
+        p, box, bl = _brio_wu_blocks(int(sizes[b]), precision, 8, local, reference_physics)
+        blist.append(box)
         blocks.extend(bl)
         params = p
     if params is None:  # a rank with no boxes
-        params, _, _ = _brio_wu_blocks(int(n_lo), precision, 8, 0)
+        params, _, _ = _brio_wu_blocks(int(n_lo), precision, 8, 0, reference_physics)
     params.h_max = 0.0
-    return _workload("brio_wu_ensemble", params, boxes, {abi.SPECIES_DEFAULT: LatticeInit(blocks)}, 100,
-                     {"sizes": sizes.tolist(), "seed": seed, "global_boxes": mine.tolist()})
+    return _workload("brio_wu_ensemble", params, blist, {abi.SPECIES_DEFAULT: LatticeInit(blocks)}, 100,
+                     {"sizes": sizes.tolist(), "seed": seed, "global_boxes": mine.tolist(),
+                      "reference_physics": bool(reference_physics)})
 
 
 def kelvin_helmholtz(n_outer=224, n_band=282, precision=abi.PREC_FP32_COMP, hfact=1.45, seed=3):

@@ -54,3 +54,50 @@ def test_checkpoint_resume_continues_the_run(tmp_path):
     assert np.max(np.abs(got.pos - ref.pos)) <= 1e-12
     assert np.max(np.abs(got.vel - ref.vel)) <= 1e-10
     assert np.max(np.abs(got.B - ref.B)) <= 1e-10
+
+
+class _FakeContext:
+    """Stands in for a Context on the host: a clock and sums that move per step."""
+
+    def __init__(self):
+        self.steps = 0
+
+    def step(self, k, dt=0.0):
+        self.steps += k
+
+    def reduce(self):
+        n = self.steps
+        return {"steps": n, "time": 0.01 * n, "dt": 0.01, "dt_next": 0.01, "e_kin": 1.0 + n, "e_int": 2.0,
+                "e_mag": 0.5, "mom": [0.0, 1e-3 * n, 0.0], "divb_mean": 1e-4, "divb_max": 1e-3, "c_h": 2.0,
+                "pairs": 1000.0 * n, "replays": 0}
+
+    def timings(self):
+        return [0.1, 0.2, 0.3, 0.05, 0.7]
+
+
+def test_diagnostics_log_lines(tmp_path):
+    path = str(tmp_path / "diag.jsonl")
+    rows = io.run_logged(_FakeContext(), 7, path, every=3, meta={"workload": "fake"})
+    assert [r["step"] for r in rows] == [3, 6, 7]
+    header, back = io.read_diagnostics(path)
+    assert header["format"] == io.DIAG_FORMAT and header["workload"] == "fake"
+    assert back == rows
+    r = back[-1]
+    assert r["e_tot"] == pytest.approx(8.0 + 2.0 + 0.5)
+    assert r["mom"] == [0.0, 0.007, 0.0]
+    assert r["density_ms"] == 0.2 and r["call_ms"] == 0.7
+    with pytest.raises(ValueError):
+        (tmp_path / "bad.jsonl").write_text('{"format": "other"}\n')
+        io.read_diagnostics(str(tmp_path / "bad.jsonl"))
+
+
+@pytest.mark.gpu
+def test_diagnostics_log_of_a_run(tmp_path):
+    import spearhed_b200 as sb
+    w = setups.sod_small(scale=0.5)
+    ctx = sb.context_for(w)
+    rows = io.run_logged(ctx, 6, str(tmp_path / "sod.jsonl"), every=2)
+    ctx.close()
+    assert [r["step"] for r in rows] == [2, 4, 6]
+    assert all(r["pairs"] > 0 and r["call_ms"] > 0 for r in rows)
+    assert rows[-1]["time"] > rows[0]["time"] > 0
