@@ -805,17 +805,16 @@ int sph_ctx::growLists(uint32_t need, bool bestEffort)
 {
     uint32_t const capN = std::max<uint32_t>(32, (need + 7) & ~7u);
     SPH_CUDA_TRY(cudaStreamSynchronize(stream));
+    uint32_t* list = nullptr;
     if(bestEffort)
     {
-        // headroom only: the new rows must fit beside the old ones, else the
-        // context keeps the lists it has
-        void* probe = nullptr;
-        if(cudaMalloc(&probe, size_t(n) * capN * sizeof(uint32_t)) != cudaSuccess)
+        // headroom only: the new rows are allocated beside the old ones, and a
+        // context that cannot have them keeps the lists it has
+        if(alloc(list, size_t(n) * capN) != SPH_OK)
         {
             cudaGetLastError();
             return SPH_OK;
         }
-        cudaFree(probe);
     }
     if(dc.lists.list)
     {
@@ -827,10 +826,12 @@ int sph_ctx::growLists(uint32_t need, bool bestEffort)
         }
         dc.lists.list = nullptr;
     }
-    uint32_t* list = nullptr;
-    int st = alloc(list, size_t(n) * capN);
-    if(st)
-        return st;
+    if(!list)
+    {
+        int const st = alloc(list, size_t(n) * capN);
+        if(st)
+            return st;
+    }
     dc.lists.list = list;
     dc.lists.cap = capN;
     dropGraphs();

@@ -162,7 +162,7 @@ namespace
         for(int a = 0; a < 3; ++a)
         {
             int const ca = sph::cellCoord(B, a, pos[a]);
-            rel[a] = pos[a] - (B.lo[a] + double(ca) * B.edge[a]);
+            rel[a] = __dsub_rn(pos[a], cellOrigin(B, a, ca));
         }
         pm[p] = sph::mk4<V4>(rel[0], rel[1], rel[2], m[q]);
         hc[p] = T(h[q]);

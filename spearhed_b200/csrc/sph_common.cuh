@@ -62,6 +62,14 @@ namespace sph
         return f < 0.0 ? 0 : (f >= double(b.n[a]) ? b.n[a] - 1 : int(f));
     }
 
+    //! Lower corner of cell c on axis a, lo + c * edge with the product and the
+    //! sum rounded separately (no contraction), as the oracle computes it: the
+    //! FP32 cell-relative positions then round from the same FP64 values.
+    __device__ __forceinline__ double cellOrigin(BoxDev const& b, int a, int c)
+    {
+        return __dadd_rn(b.lo[a], __dmul_rn(double(c), b.edge[a]));
+    }
+
     //! Stencil slot 0..26 <-> offset (ox, oy, oz), x fastest; slot 13 is the centre.
     __host__ __device__ __forceinline__ int stencilOff(int slot, int a)
     {

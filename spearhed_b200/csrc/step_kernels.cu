@@ -17,7 +17,10 @@ namespace sph
     {
         constexpr int kThreads = 256;
 
-        //! Drift (Movable): x += v dt with periodic wrap; then the cell key.
+        //! Drift (Movable): x += v dt with periodic wrap; then the cell key.  The
+        //! product and the sum are rounded separately, as the reference's CPU
+        //! path evaluates PushVelocity (PushVelocity.hpp:38-41), so the FP64
+        //! positions equal the oracle's bit for bit.
         //! Key = 2 * global cell + (0 for targets, 1 for other sources); particles
         //! that are no source sort behind every cell (key 2 * ncells).
         __global__ void __launch_bounds__(kThreads) kDriftKeys(DevCtx c, bool drift)
@@ -37,7 +40,7 @@ namespace sph
                 x[a] = c.cur.x[a][p];
                 if(drift && (role & SPH_ROLE_MOVABLE))
                 {
-                    x[a] += c.cur.v[a][p] * dt;
+                    x[a] = __dadd_rn(x[a], __dmul_rn(c.cur.v[a][p], dt));
                     if(B.periodic[a])
                     {
                         double const hiEdge = B.lo[a] + B.L[a];
@@ -84,7 +87,7 @@ namespace sph
 #pragma unroll
                         for(int a = 0; a < 3; ++a)
                         {
-                            double const rel = x[a] - (B.lo[a] + double(cc[a]) * B.edge[a]);
+                            double const rel = __dsub_rn(x[a], cellOrigin(B, a, cc[a]));
                             uint32_t const s = B.m[a] == 2 && rel >= 0.5 * B.edge[a] ? 1u : 0u;
                             sub += s * stride;
                             stride *= uint32_t(B.m[a]);
@@ -162,7 +165,7 @@ namespace sph
             for(int a = 0; a < 3; ++a)
             {
                 int const ca = cellCoord(B, a, x[a]);
-                rel[a] = x[a] - (B.lo[a] + double(ca) * B.edge[a]);
+                rel[a] = __dsub_rn(x[a], cellOrigin(B, a, ca));
             }
             rec.pm[p] = mk4<V4>(rel[0], rel[1], rel[2], m);
             rec.hc[p] = T(h);
@@ -275,23 +278,24 @@ namespace sph
 #pragma unroll
                 for(int a = 0; a < 3; ++a)
                 {
-                    double const va = c.cur.v[a][p] + c.d.dvdt[a][p] * dt;
+                    // unfused, as EulerIntegrate.hpp:45-51 on the reference's CPU path
+                    double const va = __dadd_rn(c.cur.v[a][p], __dmul_rn(c.d.dvdt[a][p], dt));
                     c.cur.v[a][p] = va;
                     v2 += va * va;
                     acc[3 + a] += m * va;
                 }
-                double const u = c.cur.u[p] + c.d.dudt[p] * dt;
+                double const u = __dadd_rn(c.cur.u[p], __dmul_rn(c.d.dudt[p], dt));
                 c.cur.u[p] = u;
                 if(mhd)
                 {
 #pragma unroll
                     for(int a = 0; a < 3; ++a)
                     {
-                        double const Ba = c.cur.B[a][p] + c.d.dBdt[a][p] * dt;
+                        double const Ba = __dadd_rn(c.cur.B[a][p], __dmul_rn(c.d.dBdt[a][p], dt));
                         c.cur.B[a][p] = Ba;
                         B2 += Ba * Ba;
                     }
-                    c.cur.psi[p] += c.d.dpsidt[p] * dt;
+                    c.cur.psi[p] = __dadd_rn(c.cur.psi[p], __dmul_rn(c.d.dpsidt[p], dt));
                 }
                 acc[0] += 0.5 * m * v2;
                 acc[1] += m * u;

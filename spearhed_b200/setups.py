@@ -299,10 +299,12 @@ def _brio_wu_blocks(n_target, precision, nt, box_id, reference_physics=False):
     if reference_physics:
         # the reference's step: inviscid hydro, constant h and dt, no periodic
         # images (its region search has none); the pair-max cull with one h per
-        # box is the reference's global radius 2 h0 box by box
+        # box is the reference's global radius 2 h0 box by box.  The tube's free
+        # y and z surfaces expand, so the closed box leaves a tube width of room
+        # on each side.
         params = abi.default_params(kernel=abi.KERNEL_CUBIC, precision=precision, cull=abi.CULL_PAIR_MAX,
                                     physics=0, gamma=gamma, h0=1.2 * dxl, dt=1e-5)
-        box = abi.make_box((-0.75, 0.0, 0.0), (0.75, L, L), (0, 0, 0))
+        box = abi.make_box((-0.75, -L, -L), (0.75, 2.0 * L, 2.0 * L), (0, 0, 0))
         return params, box, [left, right]
     physics = (abi.PHYS_AV | abi.PHYS_MHD | abi.PHYS_DEDNER | abi.PHYS_TENSILE | abi.PHYS_CFL
                | abi.PHYS_ADAPTIVE_H)

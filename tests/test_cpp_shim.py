@@ -13,7 +13,7 @@ UpdateHydroForces<K>{}(ctx), runOneStep(ctx, n)):
     (margin 1e-6);
   - SimulationTimestep.cpp:272-330: three steps composed in one runOneStep call
     equal three single-step calls within the reference's margin 2e-5, and match
-    the oracle's three-step run (FP64 1e-12, FP32 2e-5).
+    the oracle's three-step run (FP64 1e-12, FP32 2e-5 relative).
 Expected values come from the oracle's kernel functions, which are pinned bit
 for bit to the reference's own headers (tests/test_oracle_pins.py).
 
@@ -133,12 +133,14 @@ def test_shim_timestep_composed_equals_sequential_and_oracle(shim_exe, oracle, p
     box = abi.make_box((-1, -1, -1), (1, 1, 1))
     orc = oracle.System(p, [box], abi.Species.concat(parts), np.concatenate(roles))
     orc.step(3, 0.01)
+    # FP64 to round-off; FP32 pair sums against the FP64 oracle within 2e-5
+    # relative (the wall repels the fluid to |v| ~ 64 in three steps)
     tol = 1e-12 if prec == abi.PREC_FP64 else 2e-5
     got = rows[("timestep_composed", "default")] + rows[("timestep_composed", "boundary")] + \
         rows[("timestep_composed", "tracer")]
     for i, r in enumerate(got):
-        assert r["x"] == pytest.approx(orc.s.pos[0, i], abs=tol)
-        assert r["vx"] == pytest.approx(orc.s.vel[0, i], abs=tol)
+        assert r["x"] == pytest.approx(orc.s.pos[0, i], rel=tol, abs=tol)
+        assert r["vx"] == pytest.approx(orc.s.vel[0, i], rel=tol, abs=tol)
         if i < 3:  # Default and Boundary carry rho and u
-            assert r["rho"] == pytest.approx(orc.s.density[i], abs=tol * max(1.0, abs(orc.s.density[i])))
-            assert r["u"] == pytest.approx(orc.s.u[i], abs=tol)
+            assert r["rho"] == pytest.approx(orc.s.density[i], rel=tol, abs=tol)
+            assert r["u"] == pytest.approx(orc.s.u[i], rel=tol, abs=tol)
