@@ -406,6 +406,17 @@ const char* sph_last_error_string(void);
  * usable again.  Returns the previous setting. */
 long long sphx_fail_alloc_after(long long after);
 
+/* Diagnostic hook (no reference counterpart): the cell grid box `box` ran its
+ * last neighbour build on, out[12] = cells per axis (3), cell edges (3),
+ * level-1 splits per axis (3), levels, the smallest level-1 edge, the h cap. */
+int sphx_box_grid(sph_ctx* ctx, int32_t box, double* out);
+
+/* Diagnostic hook (no reference counterpart): the FP32 pair records of one
+ * species as the last neighbour build made them, pm[4 n] in input order:
+ * position relative to the lower corner of its cell (x, y, z) and mass.
+ * FP32-compensated contexts only. */
+int sphx_get_pair_records(sph_ctx* ctx, int32_t species_id, float* pm);
+
 #ifdef __cplusplus
 }
 #endif

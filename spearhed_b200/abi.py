@@ -12,7 +12,10 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libspearhed_b200.so")
+# SPEARHED_B200_VARIANT=check loads the bounds-checked build (device index
+# checks that report SPH_ERR_STATE instead of reading out of range)
+VARIANT = os.environ.get("SPEARHED_B200_VARIANT", "")
+LIB_PATH = os.path.join(HERE, "_lib", "libspearhed_b200_check.so" if VARIANT == "check" else "libspearhed_b200.so")
 
 # status codes
 SPH_OK = 0
@@ -289,6 +292,8 @@ def lib():
         "sph_wait": (C.c_int, [ctx_p]),
         "sph_density_noalloc": (C.c_int, [P(SphParams), P(SphBox), C.c_int64] + [C.c_void_p] * 7),
         "sphx_fail_alloc_after": (C.c_longlong, [C.c_longlong]),
+        "sphx_box_grid": (C.c_int, [ctx_p, C.c_int32, P(C.c_double)]),
+        "sphx_get_pair_records": (C.c_int, [ctx_p, C.c_int32, P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

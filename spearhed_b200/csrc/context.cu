@@ -1016,6 +1016,15 @@ int sph_ctx::evalStatus(char const* where)
             SPH_ERR_OUTSIDE,
             std::string(where) + ": " + std::to_string(stat[sph::kStatOutside])
                 + " particles outside their box (a non-periodic axis, or a periodic one they were not wrapped on)");
+    if(stat[sph::kStatCheck])
+    {
+        char bits[16];
+        std::snprintf(bits, sizeof(bits), "0x%x", stat[sph::kStatCheck]);
+        return fail(
+            SPH_ERR_STATE,
+            std::string(where) + ": a device bounds check failed (sites " + bits
+                + "; the access was skipped and the results are not valid)");
+    }
     if(stat[sph::kStatOverflow])
         return fail(
             SPH_ERR_OVERFLOW,
@@ -1749,6 +1758,55 @@ int sph_step(sph_ctx* ctx, int32_t n_steps, double dt)
     BoundedCall const bounded(ctx);
     sph::NvtxRange const range("sph_step");
     return ctx->steps(n_steps, dt);
+}
+
+int sphx_box_grid(sph_ctx* ctx, int32_t box, double* out)
+{
+    if(!ctx || !out || box < 0 || uint32_t(box) >= ctx->dc.nbox || !ctx->allocated)
+        return fail(SPH_ERR_INVALID, "sphx_box_grid: bad arguments");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    SPH_COMPLETE_PENDING(ctx);
+    sph::BoxDev b{};
+    SPH_CUDA_TRY(cudaMemcpyAsync(&b, ctx->dc.boxes + box, sizeof(b), cudaMemcpyDeviceToHost, ctx->stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for(int a = 0; a < 3; ++a)
+    {
+        out[a] = double(b.n[a]);
+        out[3 + a] = b.edge[a];
+        out[6 + a] = double(b.m[a]);
+    }
+    out[9] = double(b.levels);
+    out[10] = b.e1;
+    out[11] = b.hcap;
+    return SPH_OK;
+}
+
+int sphx_get_pair_records(sph_ctx* ctx, int32_t species_id, float* pm)
+{
+    if(!ctx || !pm || species_id < 0 || species_id >= SPH_NUM_SPECIES || !ctx->allocated
+       || ctx->p.precision != SPH_PREC_FP32_COMP)
+        return fail(SPH_ERR_INVALID, "sphx_get_pair_records: bad arguments (FP32 contexts only)");
+    SPH_CUDA_TRY(cudaSetDevice(ctx->p.device));
+    SPH_COMPLETE_PENDING(ctx);
+    HostSpecies const& s = ctx->sp[species_id];
+    uint32_t const n = ctx->n;
+    std::vector<float4> rec(n);
+    std::vector<uint32_t> id(n);
+    SPH_CUDA_TRY(cudaMemcpyAsync(rec.data(), ctx->dc.r32.pm, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(id.data(), ctx->dc.cur.id, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for(uint32_t p = 0; p < n; ++p)
+    {
+        int64_t const k = int64_t(id[p]) - s.offset;
+        if(k < 0 || k >= s.n)
+            continue;
+        pm[4 * k + 0] = rec[p].x;
+        pm[4 * k + 1] = rec[p].y;
+        pm[4 * k + 2] = rec[p].z;
+        pm[4 * k + 3] = rec[p].w;
+    }
+    return SPH_OK;
 }
 
 long long sphx_fail_alloc_after(long long after)

@@ -75,6 +75,42 @@ namespace sph
             return c.shift64 + size_t(box) * 32;
         }
 
+        //! Paired FP32 arithmetic (sm_100 f32x2) that rounds like the reference's
+        //! unfused scalar x, y, z sum.  A paired multiply feeding a paired add is
+        //! contracted into a fused multiply-add even when both are written in
+        //! PTX with an explicit .rn (measured on sm_100a: r^2 then differs from
+        //! the scalar __fmul_rn/__fadd_rn sum by one ulp, which moves pairs at
+        //! r^2 = R^2 across the cull).  Squares are therefore formed as
+        //! fma.rn(a, a, zero) with a zero the compiler cannot see (one computed
+        //! from a kernel argument): that is round(a^2) exactly, and an add of
+        //! two fused results has nothing left to contract.
+        __device__ __forceinline__ float2 add2Rn(float2 a, float2 b)
+        {
+            unsigned long long r;
+            asm("add.rn.f32x2 %0, %1, %2;"
+                : "=l"(r)
+                : "l"(*reinterpret_cast<unsigned long long const*>(&a)),
+                  "l"(*reinterpret_cast<unsigned long long const*>(&b)));
+            return *reinterpret_cast<float2 const*>(&r);
+        }
+        __device__ __forceinline__ float2 sq2Rn(float2 a, float2 zero)
+        {
+            unsigned long long r;
+            asm("fma.rn.f32x2 %0, %1, %1, %2;"
+                : "=l"(r)
+                : "l"(*reinterpret_cast<unsigned long long const*>(&a)),
+                  "l"(*reinterpret_cast<unsigned long long const*>(&zero)));
+            return *reinterpret_cast<float2 const*>(&r);
+        }
+        //! A run-time zero: R * 0 with R a finite kernel argument.  IEEE
+        //! arithmetic does not let the compiler fold it (R could be NaN or
+        //! infinite), so it stays opaque to contraction.
+        __device__ __forceinline__ float2 opaqueZero2(float R)
+        {
+            float const z = __fmul_rn(R, 0.0f);
+            return make_float2(z, z);
+        }
+
         // Unfused arithmetic: the reference's CPU evaluation of the pair geometry.
         __device__ __forceinline__ float mulRn(float a, float b)
         {
@@ -267,6 +303,7 @@ namespace sph
             float2 const oy = make_float2(own.y, own.y);
             float2 const oz = make_float2(own.z, own.z);
             float2 const nR2 = make_float2(-R2g, -R2g);
+            float2 const zero = opaqueZero2(supT);
             uint32_t mask = 0;
 #pragma unroll
             for(int q = 0; q < 32; q += 4)
@@ -280,10 +317,10 @@ namespace sph
 #pragma unroll
                 for(int p = 0; p < 2; ++p)
                 {
-                    float2 const dx = __fadd2_rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
-                    float2 const dy = __fadd2_rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
-                    float2 const dz = __fadd2_rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
-                    float2 const r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+                    float2 const dx = add2Rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
+                    float2 const dy = add2Rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
+                    float2 const dz = add2Rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
+                    float2 const r2 = add2Rn(add2Rn(sq2Rn(dx, zero), sq2Rn(dy, zero)), sq2Rn(dz, zero));
                     float2 nr = nR2;
                     if constexpr(PAIRMAX)
                     {
@@ -292,7 +329,7 @@ namespace sph
                         float const n0 = p ? hv.z : hv.x, n1 = p ? hv.w : hv.y;
                         nr = make_float2(fminf(nRi2, n0), fminf(nRi2, n1));
                     }
-                    float2 const d = __fadd2_rn(r2, nr);
+                    float2 const d = add2Rn(r2, nr);
                     mask = __funnelshift_l(__float_as_uint(d.x), mask, 1);
                     mask = __funnelshift_l(__float_as_uint(d.y), mask, 1);
                 }
@@ -357,20 +394,21 @@ namespace sph
             float2 const ox = make_float2(own.x, own.x);
             float2 const oy = make_float2(own.y, own.y);
             float2 const oz = make_float2(own.z, own.z);
+            float2 const zero = opaqueZero2(R2g);
 #pragma unroll
             for(int p = 0; p < 2; ++p)
             {
-                float2 const dx = __fadd2_rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
-                float2 const dy = __fadd2_rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
-                float2 const dz = __fadd2_rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
-                float2 const r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+                float2 const dx = add2Rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
+                float2 const dy = add2Rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
+                float2 const dz = add2Rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
+                float2 const r2 = add2Rn(add2Rn(sq2Rn(dx, zero), sq2Rn(dy, zero)), sq2Rn(dz, zero));
                 float2 nr = make_float2(-R2g, -R2g);
                 if constexpr(PAIRMAX)
                 {
                     float const n0 = p ? hv.z : hv.x, n1 = p ? hv.w : hv.y;
                     nr = make_float2(fminf(nRi2, n0), fminf(nRi2, n1));
                 }
-                float2 const d = __fadd2_rn(r2, nr);
+                float2 const d = add2Rn(r2, nr);
                 acc[2 * p] = d.x < 0.f;
                 acc[2 * p + 1] = d.y < 0.f;
             }
@@ -606,6 +644,8 @@ namespace sph
                 uint32_t nslot = 0;
                 auto fetch = [&](uint32_t e)
                 {
+                    if(!checkIndex((e >> 5) < c.n, c.status, kChkRowEntry))
+                        e = 0;
                     nslot = e & 31u;
                     npm = ld4(rec.pm + (e >> 5));
                 };
@@ -650,7 +690,9 @@ namespace sph
             {
                 for(int b = 0; b < kBlock && k < n; ++b, k += uint32_t(S))
                 {
-                    uint32_t const e = row[k];
+                    uint32_t e = row[k];
+                    if(!checkIndex((e >> 5) < c.n, c.status, kChkRowEntry))
+                        e = 0;
                     term(ld4(rec.pm + (e >> 5)), ld4(stab + (e & 31u)));
                 }
                 rho.fold();
@@ -734,9 +776,11 @@ namespace sph
                 uint32_t const l = q - c.boxes[box].activeBase;
                 uint32_t const nc0 = c.boxes[box].ncells;
                 uint32_t const cell = c.boxes[box].cellBase + (l < nc0 ? l : c.boxes[box].ncellsMax + (l - nc0));
+                if(!checkIndex(cell < c.cells.ncells, c.status, kChkCell))
+                    continue;
                 uint32_t const tBeg = c.cells.start[cell];
                 uint32_t const tEnd = c.cells.mid[cell];
-                if(tBeg >= tEnd)
+                if(tBeg >= tEnd || !checkIndex(tEnd <= c.n, c.status, kChkTargets))
                     continue;
                 if(box != chBox)
                 {
@@ -838,12 +882,18 @@ namespace sph
                         uint32_t const par = (uint32_t(p[2]) * uint32_t(B.n[1]) + uint32_t(p[1])) * uint32_t(B.n[0])
                                              + uint32_t(p[0]);
                         uint32_t const cellId = B.cellBase + B.ncellsMax + par * B.msub + subc;
+                        if(!checkIndex(cellId < c.cells.ncells, c.status, kChkCell))
+                            return;
                         sBeg = c.cells.start[cellId];
                         sCnt = c.cells.end[cellId] - sBeg;
+                        if(!checkIndex(sBeg <= c.n && sCnt <= c.n - sBeg, c.status, kChkRange))
+                            sCnt = 0;
                         return;
                     }
                     uint32_t const cellId
                         = B.cellBase + (uint32_t(f[2]) * uint32_t(B.n[1]) + uint32_t(f[1])) * uint32_t(B.n[0]) + uint32_t(f[0]);
+                    if(!checkIndex(cellId < c.cells.ncells, c.status, kChkCell))
+                        return;
                     if(fine)
                     {
                         // all level-1 sub-cells of a level-0 neighbour, as one range
@@ -855,6 +905,8 @@ namespace sph
                         sBeg = c.cells.start[cellId];
                         sCnt = c.cells.end[cellId] - sBeg;
                     }
+                    if(!checkIndex(sBeg <= c.n && sCnt <= c.n - sBeg, c.status, kChkRange))
+                        sCnt = 0;
                 };
 
                 // exclusive prefix of the page's source counts and the page total
@@ -959,7 +1011,7 @@ namespace sph
                                 }
                                 dsc[k] = sd;
                                 ent[k] = __shfl_sync(0xffffffffu, eBase, sd) + (q << 5);
-                                if(q < ce)
+                                if(q < ce && checkIndex((ent[k] >> 5) < c.n, c.status, kChkStaged))
                                 {
                                     pj[k] = ld4(rec.pm + (ent[k] >> 5));
                                     if constexpr(PAIRMAX)
@@ -1296,6 +1348,8 @@ namespace sph
                 uint32_t nslot = 0;
                 auto fetch = [&](uint32_t e)
                 {
+                    if(!checkIndex((e >> 5) < c.n, c.status, kChkRowEntry))
+                        e = 0;
                     uint32_t const j = e >> 5;
                     nslot = e & 31u;
                     npm = ld4(rec.pm + j);

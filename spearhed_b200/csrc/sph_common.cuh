@@ -305,6 +305,38 @@ namespace sph
         kStatNonFinite = 2,  //!< non-finite positions
         kStatMaxCount = 3,   //!< largest neighbour count seen (list sizing)
         kStatBadInput = 4,   //!< gathered h / source masses that are not positive and finite
+        kStatCheck = 5,      //!< bounds-checked builds: bit s set when the check at site s failed
         kStatWords = 8
     };
+
+    //! Sites of the device bounds checks (bits of the kStatCheck word).
+    enum CheckSite
+    {
+        kChkCell = 0,       //!< a stencil cell id within the cell arrays
+        kChkRange = 1,      //!< a cell's source range within the particles
+        kChkStaged = 2,     //!< a staged candidate's particle index
+        kChkTargets = 3,    //!< a target cell's range within the particles
+        kChkRowEntry = 4,   //!< a list entry read back (particle index and stencil slot)
+        kChkPermute = 5,    //!< a permutation index
+        kChkKey = 6,        //!< a sorted cell key within the cells
+        kChkDriftCell = 7   //!< a particle's cell id from the drift
+    };
+
+    //! Bounds-checked builds (compiled with -DSPH_CHECK): a failed check sets
+    //! its site's bit in status[kStatCheck] and returns false, and the caller
+    //! skips the access, so a bad index is reported, never dereferenced.  In
+    //! the normal build every check is `true` and costs nothing.
+    __device__ __forceinline__ bool checkIndex(bool ok, uint32_t* status, int site)
+    {
+#ifdef SPH_CHECK
+        if(!ok)
+            atomicOr(&status[kStatCheck], 1u << site);
+        return ok;
+#else
+        (void)ok;
+        (void)status;
+        (void)site;
+        return true;
+#endif
+    }
 } // namespace sph

@@ -94,7 +94,8 @@ namespace sph
                         }
                         cell = B.cellBase + B.ncellsMax + (cell - B.cellBase) * B.msub + sub;
                     }
-                    key = 2u * cell + (isTarget(role) ? 0u : 1u);
+                    if(checkIndex(cell < c.cells.ncells, c.status, kChkDriftCell))
+                        key = 2u * cell + (isTarget(role) ? 0u : 1u);
                 }
             }
             c.keysA[p] = key;
@@ -135,6 +136,8 @@ namespace sph
             if(p >= c.n)
                 return;
             uint32_t const q = perm[p];
+            if(!checkIndex(q < c.n, c.status, kChkPermute))
+                return;
             double x[3], v[3], Bv[3];
 #pragma unroll
             for(int a = 0; a < 3; ++a)
