@@ -727,7 +727,7 @@ def run_ours(args, rank, world):
                    "parallelism": (f"box_shards{world}" if sharded else f"replicas{world}") if world > 1 else "single",
                    "l2": l2_note, "graph": bool(args.graph),
                    "launch_shapes": {k: tune[k] for k in ("staging_depth", "density_blocks_per_sm",
-                                                          "force_blocks_per_sm", "steps_per_trial",
+                                                          "cull_unroll", "force_blocks_per_sm", "steps_per_trial",
                                                           "density_ms", "force_ms")}},
         "stage_ms_per_step": stage_dict(tm, args.steps),
         "fp64_plain": fp64,

@@ -279,8 +279,8 @@ int sph_prepare_graph(sph_ctx* ctx);
 /* Launch shapes of the two pair kernels (no reference counterpart; the
  * reference's frame size and threads per frame are compile-time constants,
  * spmacc/Frame.hpp:49-132).  density: staging depth (candidates per shared-memory
- * window) and register cap (blocks per SM); force: register cap.  Every shape
- * gives identical bits. */
+ * window), register cap (blocks per SM) and, in FP32, the unroll depth of the
+ * mask cull; force: register cap.  Every shape gives identical bits. */
 typedef struct SphTuning
 {
     int32_t density_variant;      /* index into the density shapes (0 = default)          */
@@ -293,6 +293,8 @@ typedef struct SphTuning
     int32_t steps_per_trial;      /* steps timed per shape by sph_autotune (0: not tuned)  */
     double density_ms[8];         /* per-step density time of each shape (sph_autotune)   */
     double force_ms[8];           /* per-step force time of each shape (sph_autotune)     */
+    int32_t cull_unroll;          /* FP32 density: 4-candidate groups of the 32-candidate
+                                     mask cull unrolled (8 = all, 2); 0 in FP64          */
 } SphTuning;
 
 /* Times every launch shape of the density and force kernels on this context's

@@ -237,6 +237,7 @@ class SphTuning(C.Structure):
         ("steps_per_trial", C.c_int32),
         ("density_ms", C.c_double * 8),
         ("force_ms", C.c_double * 8),
+        ("cull_unroll", C.c_int32),
     ]
 
     def as_dict(self):

@@ -1168,7 +1168,8 @@ void sph_ctx::describeTuning()
 {
     tuning.density_variant = densityVariant;
     tuning.force_variant = forceVariant;
-    sph::densityShape(p.precision, densityVariant, &tuning.staging_depth, &tuning.density_blocks_per_sm);
+    sph::densityShape(p.precision, densityVariant, &tuning.staging_depth, &tuning.density_blocks_per_sm,
+                      &tuning.cull_unroll);
     tuning.force_blocks_per_sm = sph::forceBlocksPerSm(p.precision, int(p.physics), forceVariant);
     tuning.n_density_variants = sph::densityVariants(p.precision);
     tuning.n_force_variants = sph::forceVariants(p.precision);

@@ -288,7 +288,10 @@ namespace sph
         //! negative exactly when r^2 < R^2, and funnels it into the mask.
         //! FP32: two candidates per instruction with the paired f32x2 arithmetic
         //! of sm_100 (round-to-nearest per element, the scalar rounding).
-        template<bool PAIRMAX>
+        //! UNR: how many of the eight 4-candidate groups the compiler unrolls
+        //! (8 = all; 2 keeps the hot code small where warps run several phases
+        //! at once and the instruction caches become the bound).
+        template<bool PAIRMAX, int UNR>
         __device__ __forceinline__ uint32_t cullMask32(
             float4 const& own,
             float nRi2,
@@ -305,7 +308,7 @@ namespace sph
             float2 const nR2 = make_float2(-R2g, -R2g);
             float2 const zero = opaqueZero2(supT);
             uint32_t mask = 0;
-#pragma unroll
+#pragma unroll UNR
             for(int q = 0; q < 32; q += 4)
             {
                 float4 const xv = *reinterpret_cast<float4 const*>(X + q);
@@ -337,7 +340,7 @@ namespace sph
             return mask;
         }
 
-        template<bool PAIRMAX>
+        template<bool PAIRMAX, int UNR>
         __device__ __forceinline__ uint32_t cullMask32(
             D4 const& own,
             double nRi2,
@@ -490,7 +493,7 @@ namespace sph
         //! The staging holds negated shifted positions (sNX, sNY, sNZ), so
         //! dx = x_i + (-x_j) is the reference's x_i - x_j, rounding included; the
         //! window is padded with far candidates up to a multiple of 32.
-        template<typename V4, typename T, bool PAIRMAX>
+        template<typename V4, typename T, bool PAIRMAX, int UNR>
         __device__ __forceinline__ void cullChunk(
             TargetChunk<V4, T>& ch,
             T const* sNX,
@@ -517,7 +520,7 @@ namespace sph
                 for(uint32_t q0 = 0; q0 < m; q0 += 32)
                 {
                     uint32_t mask
-                        = cullMask32<PAIRMAX>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
+                        = cullMask32<PAIRMAX, UNR>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
                     if(!ch.act)
                         mask = 0;
                     if(countOnly)
@@ -675,15 +678,13 @@ namespace sph
                         rho.fold();
                     qc = qn;
                 }
+                // the last 1-3 entries (qc.x already fetched); a loop that is not
+                // unrolled keeps one copy of the term, and the fetch after the
+                // last entry re-reads qc.x, a valid entry
                 uint32_t const tail = n - nFull;
-                if(tail > 0)
-                {
-                    step(tail > 1 ? qc.y : qc.x);
-                    if(tail > 1)
-                        step(tail > 2 ? qc.z : qc.y);
-                    if(tail > 2)
-                        step(qc.z);
-                }
+#pragma unroll 1
+                for(uint32_t i = 0; i < tail; ++i)
+                    step(i + 1 < tail ? (i == 0 ? qc.y : qc.z) : qc.x);
             }
             uint32_t k = S == 1 ? n : uint32_t(ch.sub);
             while(k < n)
@@ -732,8 +733,9 @@ namespace sph
 
         //! Tunable launch shapes (picked per context by sph_autotune): CAP is the
         //! staging depth (candidates per shared-memory window), MINB the blocks
-        //! per SM the register allocation must admit.
-        template<int K, typename T, bool PAIRMAX, int CAP, int MINB>
+        //! per SM the register allocation must admit, CU the unroll depth of the
+        //! FP32 mask cull (8 or 2; the FP64 cull ignores it).
+        template<int K, typename T, bool PAIRMAX, int CAP, int MINB, int CU>
         __global__ void __launch_bounds__(kDensWarps * 32, MINB) kDensity(DevCtx c, PhysArgs pa, bool countOnly)
         {
             using V4 = typename PairCfg<T>::V4;
@@ -1064,11 +1066,20 @@ namespace sph
                                 sH[q] = T(0);
                         }
                         __syncwarp();
-                        cullChunk<V4, T, PAIRMAX>(
-                            A, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
-                        if(twoChunks)
-                            cullChunk<V4, T, PAIRMAX>(
-                                Bc, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                        // One copy of the cull serves both chunks (a loop that is not
+                        // unrolled): the kernel's hot code stays small enough for the
+                        // instruction caches when warps run different phases at once.
+#pragma unroll 1
+                        for(int w = 0; w < (twoChunks ? 2 : 1); ++w)
+                        {
+                            TargetChunk<V4, T> ch = w ? Bc : A;
+                            cullChunk<V4, T, PAIRMAX, CU>(
+                                ch, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                            if(w)
+                                Bc = ch;
+                            else
+                                A = ch;
+                        }
                         cand += uint64_t(m) * nTargets;
                     }
                     }
@@ -1090,9 +1101,13 @@ namespace sph
                         flushChunk(Bc, c.lists.list, cap);
                     __syncwarp();
                     V4 const* const stab = shiftTable<T>(c, box);
-                    chMax = fmax(chMax, densityChunk<K>(A, c, rec, pa, stab, cap));
-                    if(twoChunks)
-                        chMax = fmax(chMax, densityChunk<K>(Bc, c, rec, pa, stab, cap));
+                    // one copy of the density sum and its epilogue for both chunks
+#pragma unroll 1
+                    for(int w = 0; w < (twoChunks ? 2 : 1); ++w)
+                    {
+                        TargetChunk<V4, T> const ch = w ? Bc : A;
+                        chMax = fmax(chMax, densityChunk<K>(ch, c, rec, pa, stab, cap));
+                    }
                 }
             }
             maxCount = warpMaxU(maxCount);
@@ -1388,15 +1403,13 @@ namespace sph
                     qc = qn;
                 }
                 // tail: the first n - nFull entries of qc, its first already fetched
+                // the last 1-3 entries (qc.x already fetched); a loop that is not
+                // unrolled keeps one copy of the term, and the fetch after the
+                // last entry re-reads qc.x, a valid entry
                 uint32_t const tail = n - nFull;
-                if(tail > 0)
-                {
-                    step(tail > 1 ? qc.y : qc.x);
-                    if(tail > 1)
-                        step(tail > 2 ? qc.z : qc.y);
-                    if(tail > 2)
-                        step(qc.z);
-                }
+#pragma unroll 1
+                for(uint32_t i = 0; i < tail; ++i)
+                    step(i + 1 < tail ? (i == 0 ? qc.y : qc.z) : qc.x);
                 A.fold();
                 dtLocal = forceEpilogue<T, PH>(c, pa, t, myBox, A, own.dedner);
             }
@@ -1419,12 +1432,14 @@ namespace sph
         }
 
         // ---- launch-shape variants -------------------------------------------
-        // density FP32: (CAP, blocks/SM) = (256, 6), (256, 5), (128, 6), (128, 5);
+        // density FP32: (CAP, blocks/SM) = (256, 6), (256, 5), (128, 6), (128, 5),
+        // each with the mask cull fully unrolled and unrolled twice;
         // density FP64: (256, 4), (128, 4).  force FP32: 4 or 5 blocks/SM (SPMHD
         // default 4, hydro default 5); force FP64: 3.  Variant 0 is the default.
-        constexpr int kDensVariants32 = 4, kDensVariants64 = 2, kForceVariants32 = 2, kForceVariants64 = 1;
-        constexpr int kDensCap32[kDensVariants32] = {256, 256, 128, 128};
-        constexpr int kDensBlk32[kDensVariants32] = {6, 5, 6, 5};
+        constexpr int kDensVariants32 = 8, kDensVariants64 = 2, kForceVariants32 = 2, kForceVariants64 = 1;
+        constexpr int kDensCap32[kDensVariants32] = {256, 256, 128, 128, 256, 256, 128, 128};
+        constexpr int kDensBlk32[kDensVariants32] = {6, 5, 6, 5, 6, 5, 6, 5};
+        constexpr int kDensUnr32[kDensVariants32] = {8, 8, 8, 8, 2, 2, 2, 2};
         constexpr int kDensCap64[kDensVariants64] = {256, 128};
 
         //! Shared-memory carve-out (percent of the maximum) that fits `blocks`
@@ -1438,10 +1453,10 @@ namespace sph
             return pct > 100 ? 100 : pct;
         }
 
-        template<int K, typename T, bool PM, int CAP, int MINB>
+        template<int K, typename T, bool PM, int CAP, int MINB, int CU = 8>
         void configureDensity()
         {
-            auto f = kDensity<K, T, PM, CAP, MINB>;
+            auto f = kDensity<K, T, PM, CAP, MINB, CU>;
             size_t const smem = densitySmem<T, PM, CAP>();
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carveout(smem, MINB));
@@ -1453,7 +1468,7 @@ namespace sph
             cudaFuncSetAttribute(kForce<K, T, PH, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
         }
 
-        template<int K, typename T, bool PM, int CAP, int MINB>
+        template<int K, typename T, bool PM, int CAP, int MINB, int CU = 8>
         void densityLaunch(DevCtx const& c, PhysArgs const& pa, bool countOnly, cudaStream_t s)
         {
             size_t const smem = densitySmem<T, PM, CAP>();
@@ -1465,7 +1480,7 @@ namespace sph
             if(blocks)
             {
                 cudaMemsetAsync(c.work, 0, sizeof(uint32_t), s);
-                kDensity<K, T, PM, CAP, MINB><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
+                kDensity<K, T, PM, CAP, MINB, CU><<<blocks, kDensWarps * 32, smem, s>>>(c, pa, countOnly);
                 countLaunches(1);
             }
         }
@@ -1477,10 +1492,16 @@ namespace sph
             {
                 switch(variant)
                 {
-                case 1: densityLaunch<K, T, PM, kDensCap32[1], kDensBlk32[1]>(c, pa, countOnly, s); break;
-                case 2: densityLaunch<K, T, PM, kDensCap32[2], kDensBlk32[2]>(c, pa, countOnly, s); break;
-                case 3: densityLaunch<K, T, PM, kDensCap32[3], kDensBlk32[3]>(c, pa, countOnly, s); break;
-                default: densityLaunch<K, T, PM, kDensCap32[0], kDensBlk32[0]>(c, pa, countOnly, s); break;
+#define SPH_DENS32(v) densityLaunch<K, T, PM, kDensCap32[v], kDensBlk32[v], kDensUnr32[v]>(c, pa, countOnly, s)
+                case 1: SPH_DENS32(1); break;
+                case 2: SPH_DENS32(2); break;
+                case 3: SPH_DENS32(3); break;
+                case 4: SPH_DENS32(4); break;
+                case 5: SPH_DENS32(5); break;
+                case 6: SPH_DENS32(6); break;
+                case 7: SPH_DENS32(7); break;
+                default: SPH_DENS32(0); break;
+#undef SPH_DENS32
                 }
             }
             else
@@ -1560,10 +1581,16 @@ namespace sph
         template<int K, bool PM>
         void configureDensityK()
         {
-            configureDensity<K, float, PM, kDensCap32[0], kDensBlk32[0]>();
-            configureDensity<K, float, PM, kDensCap32[1], kDensBlk32[1]>();
-            configureDensity<K, float, PM, kDensCap32[2], kDensBlk32[2]>();
-            configureDensity<K, float, PM, kDensCap32[3], kDensBlk32[3]>();
+#define SPH_CONF32(v) configureDensity<K, float, PM, kDensCap32[v], kDensBlk32[v], kDensUnr32[v]>()
+            SPH_CONF32(0);
+            SPH_CONF32(1);
+            SPH_CONF32(2);
+            SPH_CONF32(3);
+            SPH_CONF32(4);
+            SPH_CONF32(5);
+            SPH_CONF32(6);
+            SPH_CONF32(7);
+#undef SPH_CONF32
             configureDensity<K, double, PM, kDensCap64[0], 4>();
             configureDensity<K, double, PM, kDensCap64[1], 4>();
         }
@@ -1610,12 +1637,13 @@ namespace sph
         return precision == SPH_PREC_FP64 ? kForceVariants64 : kForceVariants32;
     }
 
-    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm)
+    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm, int* cullUnroll)
     {
         bool const f64 = precision == SPH_PREC_FP64;
         int const v = variant < 0 || variant >= densityVariants(precision) ? 0 : variant;
         *stagingDepth = f64 ? kDensCap64[v] : kDensCap32[v];
         *blocksPerSm = f64 ? 4 : kDensBlk32[v];
+        *cullUnroll = f64 ? 0 : kDensUnr32[v];
     }
 
     int forceBlocksPerSm(int precision, int physics, int variant)

@@ -383,7 +383,7 @@ namespace sph
     void launchForce(DevCtx const& c, PhysArgs const& pa, int kernel, int precision, int variant, cudaStream_t s);
     int densityVariants(int precision);
     int forceVariants(int precision);
-    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm);
+    void densityShape(int precision, int variant, int* stagingDepth, int* blocksPerSm, int* cullUnroll);
     int forceBlocksPerSm(int precision, int physics, int variant);
     //! Sets the shared-memory attributes of every pair-kernel instantiation
     //! (once, before any launch, so no attribute call happens during a graph capture).

@@ -1,6 +1,6 @@
 """Launch-shape tuning of the pair kernels.
 
-- Every shape (staging depth, register caps) gives the same bits as the
+- Every shape (staging depth, register caps, cull unroll) gives the same bits as the
   default: the shapes change windows and register allocation, not arithmetic
   or summation order.
 - sph_autotune leaves the particles, the clock and the step count as they were,
@@ -63,6 +63,7 @@ def test_autotune_keeps_the_state():
     assert all(x > 0 for x in t["density_ms"] + t["force_ms"])
     assert 0 <= t["density_variant"] < t["n_density_variants"]
     assert t["staging_depth"] in (128, 256)
+    assert t["cull_unroll"] in ((8, 2) if t["n_density_variants"] == 8 else (0,))
     # the context keeps stepping with the chosen shapes
     ctx.step(1)
     assert ctx.reduce()["steps"] == 3
