@@ -375,73 +375,6 @@ namespace sph
             return mask;
         }
 
-        //! Acceptance of four consecutive staged candidates for one target (the
-        //! short-chunk path): the same rounded r^2 - R^2 sign test as cullMask32.
-        template<bool PAIRMAX>
-        __device__ __forceinline__ void cull4(
-            float4 const& own,
-            float nRi2,
-            float const* X,
-            float const* Y,
-            float const* Z,
-            float const* H,
-            float R2g,
-            bool acc[4])
-        {
-            float4 const xv = *reinterpret_cast<float4 const*>(X);
-            float4 const yv = *reinterpret_cast<float4 const*>(Y);
-            float4 const zv = *reinterpret_cast<float4 const*>(Z);
-            float4 hv = make_float4(0.f, 0.f, 0.f, 0.f);
-            if constexpr(PAIRMAX)
-                hv = *reinterpret_cast<float4 const*>(H);
-            float2 const ox = make_float2(own.x, own.x);
-            float2 const oy = make_float2(own.y, own.y);
-            float2 const oz = make_float2(own.z, own.z);
-            float2 const zero = opaqueZero2(R2g);
-#pragma unroll
-            for(int p = 0; p < 2; ++p)
-            {
-                float2 const dx = add2Rn(ox, p ? make_float2(xv.z, xv.w) : make_float2(xv.x, xv.y));
-                float2 const dy = add2Rn(oy, p ? make_float2(yv.z, yv.w) : make_float2(yv.x, yv.y));
-                float2 const dz = add2Rn(oz, p ? make_float2(zv.z, zv.w) : make_float2(zv.x, zv.y));
-                float2 const r2 = add2Rn(add2Rn(sq2Rn(dx, zero), sq2Rn(dy, zero)), sq2Rn(dz, zero));
-                float2 nr = make_float2(-R2g, -R2g);
-                if constexpr(PAIRMAX)
-                {
-                    float const n0 = p ? hv.z : hv.x, n1 = p ? hv.w : hv.y;
-                    nr = make_float2(fminf(nRi2, n0), fminf(nRi2, n1));
-                }
-                float2 const d = add2Rn(r2, nr);
-                acc[2 * p] = d.x < 0.f;
-                acc[2 * p + 1] = d.y < 0.f;
-            }
-        }
-
-        template<bool PAIRMAX>
-        __device__ __forceinline__ void cull4(
-            D4 const& own,
-            double nRi2,
-            double const* X,
-            double const* Y,
-            double const* Z,
-            double const* H,
-            double R2g,
-            bool acc[4])
-        {
-#pragma unroll
-            for(int u = 0; u < 4; ++u)
-            {
-                double const dx = __dadd_rn(own.x, X[u]);
-                double const dy = __dadd_rn(own.y, Y[u]);
-                double const dz = __dadd_rn(own.z, Z[u]);
-                double const r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                double nR2 = -R2g;
-                if constexpr(PAIRMAX)
-                    nR2 = fmin(nRi2, H[u]);
-                acc[u] = __dadd_rn(r2, nR2) < 0.0;
-            }
-        }
-
         //! Per-lane state of one chunk of up to 32 targets of a cell.
         template<typename V4, typename T>
         struct TargetChunk
@@ -452,7 +385,6 @@ namespace sph
             uint32_t t;        //!< sorted target index
             uint32_t nl;       //!< accepted so far (same on every lane of the target's group)
             uint4 buf;         //!< full chunks: the last (nl mod 4) accepted entries, newest in w
-            uint32_t groupBase, groupMask, subBelow;
             int S, sub;
             bool act;
         };
@@ -470,9 +402,6 @@ namespace sph
             ch.S = subLanes(nt == 0 ? 32u : nt);
             ch.sub = lane & (ch.S - 1);
             uint32_t const tt = uint32_t(lane) / uint32_t(ch.S);
-            ch.groupBase = tt * uint32_t(ch.S);
-            ch.groupMask = ch.S == 32 ? 0xffffffffu : (((1u << ch.S) - 1u) << ch.groupBase);
-            ch.subBelow = (1u << ch.sub) - 1u;
             ch.act = tt < nt;
             ch.t = tc + tt;
             ch.nl = 0;
@@ -501,6 +430,8 @@ namespace sph
             T const* sNZ,
             T const* sH,
             uint32_t const* sEnt,
+            uint32_t const* sSelf,
+            uint32_t tc,
             uint32_t m,
             T supT,
             T R2g,
@@ -509,64 +440,53 @@ namespace sph
             bool countOnly)
         {
             uint32_t* const row = list + size_t(ch.t) * cap;
-            // the target itself: its own entry (centre slot), accepted once at r = 0
-            uint32_t const selfEnt = packEntry(ch.t, kCentreSlot);
-            if(ch.S == 1)
+            // The window is far-padded to whole 32-candidate slabs.  A target has
+            // S lanes (S = 1 for a full chunk); in round r sub-lane s builds the
+            // acceptance mask of slab r S + s (all lanes of a full chunk read the
+            // same candidates: shared-memory broadcast) and clears the bit of the
+            // target's own entry (its window position, recorded at staging).  One
+            // call site of the mask cull serves both kinds of chunk, which keeps
+            // the kernel's hot code small.
+            int const S = ch.S;
+            uint32_t const selfq = ch.act ? sSelf[ch.t - tc] : ~0u;
+            uint32_t const nSlab = (m + 31u) >> 5;
+            for(uint32_t g0 = 0; g0 < nSlab; g0 += uint32_t(S))
             {
-                // Full chunk: every lane its own target; all lanes read the same
-                // 32 candidates (shared-memory broadcast) and build a 32-bit
-                // acceptance mask, then append the accepted entries other than the
-                // target's own (a count-only pass counts it; the caller takes it off).
-                for(uint32_t q0 = 0; q0 < m; q0 += 32)
+                uint32_t const g = g0 + uint32_t(ch.sub);
+                uint32_t const q0 = g << 5;
+                uint32_t mask = 0;
+                if(g < nSlab)
                 {
-                    uint32_t mask
-                        = cullMask32<PAIRMAX, UNR>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
+                    mask = cullMask32<PAIRMAX, UNR>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
                     if(!ch.act)
                         mask = 0;
+                    if(selfq - q0 < 32u)
+                        mask &= ~(0x80000000u >> (selfq - q0));
+                }
+                uint32_t const cnt = uint32_t(__popc(mask));
+                if(S == 1)
+                {
+                    // full chunk: the lane's row grows by its own entries, four at
+                    // a time (16-byte stores; rows are 32-byte aligned and cap is a
+                    // multiple of 8)
                     if(countOnly)
                     {
-                        ch.nl += uint32_t(__popc(mask));
+                        ch.nl += cnt;
                         continue;
                     }
-                    // entries go out four at a time (16-byte stores; rows are
-                    // 32-byte aligned and cap is a multiple of 8)
                     while(mask)
                     {
                         uint32_t const u = uint32_t(__clz(mask));
                         mask &= 0x7fffffffu >> u;
-                        uint32_t const e = sEnt[q0 + u];
-                        if(e == selfEnt)
-                            continue;
-                        ch.buf = make_uint4(ch.buf.y, ch.buf.z, ch.buf.w, e);
+                        ch.buf = make_uint4(ch.buf.y, ch.buf.z, ch.buf.w, sEnt[q0 + u]);
                         ++ch.nl;
                         if((ch.nl & 3u) == 0 && ch.nl <= cap)
                             *reinterpret_cast<uint4*>(row + (ch.nl - 4)) = ch.buf;
                     }
+                    continue;
                 }
-                return;
-            }
-            // Short chunk: S lanes per target; sub-lane s tests the four consecutive
-            // candidates q0 + 4s .. q0 + 4s + 3 (vector loads, paired arithmetic),
-            // and an exclusive scan of the accepted counts over the target's S
-            // lanes places the entries in candidate order.  The window is
-            // far-padded to a multiple of 32, so a block of four that starts
-            // before m is staged whole.
-            int const S = ch.S;
-            for(uint32_t q0 = 0; q0 < m; q0 += uint32_t(4 * S))
-            {
-                uint32_t const qb = q0 + uint32_t(4 * ch.sub);
-                bool acc[4] = {false, false, false, false};
-                uint4 ent = make_uint4(0, 0, 0, 0);
-                if(ch.act && qb < m)
-                {
-                    cull4<PAIRMAX>(ch.own, ch.nR2, sNX + qb, sNY + qb, sNZ + qb, sH + qb, R2g, acc);
-                    ent = *reinterpret_cast<uint4 const*>(sEnt + qb);
-                    acc[0] = acc[0] && ent.x != selfEnt;
-                    acc[1] = acc[1] && ent.y != selfEnt;
-                    acc[2] = acc[2] && ent.z != selfEnt;
-                    acc[3] = acc[3] && ent.w != selfEnt;
-                }
-                uint32_t const cnt = uint32_t(acc[0]) + uint32_t(acc[1]) + uint32_t(acc[2]) + uint32_t(acc[3]);
+                // short chunk: an exclusive scan of the accepted counts over the
+                // target's S lanes places each slab's entries in candidate order
                 uint32_t incl = cnt;
                 for(int d = 1; d < S; d <<= 1)
                 {
@@ -578,15 +498,14 @@ namespace sph
                 if(!countOnly)
                 {
                     uint32_t k = ch.nl + incl - cnt;
-                    uint32_t const e[4] = {ent.x, ent.y, ent.z, ent.w};
-#pragma unroll
-                    for(int u = 0; u < 4; ++u)
-                        if(acc[u])
-                        {
-                            if(k < cap)
-                                row[k] = e[u];
-                            ++k;
-                        }
+                    while(mask)
+                    {
+                        uint32_t const u = uint32_t(__clz(mask));
+                        mask &= 0x7fffffffu >> u;
+                        if(k < cap)
+                            row[k] = sEnt[q0 + u];
+                        ++k;
+                    }
                 }
                 ch.nl += total;
             }
@@ -750,6 +669,10 @@ namespace sph
             T* const sH = sNZ + kDensWarps * CAP; // only with PAIRMAX: -(supT h_j)^2
             uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
                                    + warp * CAP;
+            // per warp: window position of each target's own entry (up to 64
+            // targets of the chunk pair; ~0 = not in this window)
+            uint32_t* const sSelf = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
+                                    + kDensWarps * CAP + warp * 64;
             Records<V4, T> const rec = records<T>(c);
             T const supT = T(Kern<K>::support);
             T const Rg = mulRn(supT, T(pa.h0));
@@ -983,6 +906,8 @@ namespace sph
                     {
                         uint32_t const ce = min(total, cb + uint32_t(CAP));
                         __syncwarp();
+                        sSelf[lane] = ~0u;
+                        sSelf[lane + 32] = ~0u;
                         // Flat staging: lane l reads window positions l, l + 32, ...; the
                         // descriptor of position q is the last one whose prefix is <= q
                         // (a shuffle binary search over the page's prefixes; empty
@@ -1051,6 +976,10 @@ namespace sph
                                     sEnt[w] = ent[k];
                                     if constexpr(PAIRMAX)
                                         sH[w] = nRj;
+                                    // a target's own entry: centre slot, index among the pair's targets
+                                    uint32_t const jr = (ent[k] >> 5) - tc;
+                                    if((ent[k] & 31u) == kCentreSlot && jr < nTargets)
+                                        sSelf[jr] = w;
                                 }
                                 mW += uint32_t(__popc(passMask));
                             }
@@ -1074,7 +1003,7 @@ namespace sph
                         {
                             TargetChunk<V4, T> ch = w ? Bc : A;
                             cullChunk<V4, T, PAIRMAX, CU>(
-                                ch, sNX, sNY, sNZ, sH, sEnt, m, supT, R2g, c.lists.list, cap, countOnly);
+                                ch, sNX, sNY, sNZ, sH, sEnt, sSelf, tc, m, supT, R2g, c.lists.list, cap, countOnly);
                             if(w)
                                 Bc = ch;
                             else
@@ -1082,14 +1011,6 @@ namespace sph
                         }
                         cand += uint64_t(m) * nTargets;
                     }
-                    }
-                    if(countOnly)
-                    {
-                        // full chunks' masks counted each target's own entry once
-                        if(A.act && A.S == 1)
-                            --A.nl;
-                        if(Bc.act && Bc.S == 1)
-                            --Bc.nl;
                     }
                     bool const leadA = A.act && A.sub == 0, leadB = twoChunks && Bc.act && Bc.sub == 0;
                     maxCount = max(maxCount, max(leadA ? A.nl : 0u, leadB ? Bc.nl : 0u));
@@ -1428,7 +1349,7 @@ namespace sph
         template<typename T, bool PM, int CAP>
         constexpr size_t densitySmem()
         {
-            return size_t(kDensWarps) * CAP * ((PM ? 4 : 3) * sizeof(T) + sizeof(uint32_t));
+            return size_t(kDensWarps) * (CAP * ((PM ? 4 : 3) * sizeof(T) + sizeof(uint32_t)) + 64 * sizeof(uint32_t));
         }
 
         // ---- launch-shape variants -------------------------------------------
