@@ -419,34 +419,76 @@ namespace sph
                 p[i] = v;
         }
 
-        //! Largest h of each box's particles, as ordered bits (one atomic per warp
-        //! when the warp is in one box).
+        //! Largest and smallest h of each box's particles, as ordered bits.  A
+        //! warp walks kHmaxRun consecutive groups of 32 particles (each group one
+        //! coalesced load) and keeps a running maximum and minimum while every
+        //! particle of a group is in the warp's current box.  After the first
+        //! neighbour build the particles are box-sorted, so one pair of atomics
+        //! serves a whole run instead of every group: the boxes' 512 addresses
+        //! otherwise serialise about 2 n / 32 atomics in L2.  A group that spans
+        //! boxes falls back to per-particle atomics.
+        constexpr int kHmaxRun = 16;
         __global__ void __launch_bounds__(kThreads) kBoxHmax(DevCtx c)
         {
-            uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
-            int const box = p < c.n ? c.cur.box[p] : -1;
-            double const h = p < c.n ? c.cur.h[p] : 0.0;
-            int const box0 = __shfl_sync(0xffffffffu, box, 0);
-            if(__all_sync(0xffffffffu, box == box0 || box < 0))
+            int const lane = threadIdx.x & 31;
+            uint32_t const base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32u * kHmaxRun);
+            int cur = -1; // warp-uniform: the box the running extrema belong to
+            double m = 0.0, mn = 1e300;
+            auto flush = [&]()
             {
-                double m = box >= 0 ? h : 0.0, mn = box >= 0 ? h : 1e300;
+                if(cur < 0)
+                    return;
 #pragma unroll
                 for(int o = 16; o > 0; o >>= 1)
                 {
                     m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
                     mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
                 }
-                if((threadIdx.x & 31) == 0 && box0 >= 0)
+                if(lane == 0)
                 {
-                    atomicMax(&c.bs.hmaxBits[box0], orderedBits(m));
-                    atomicMin(&c.bs.hminBits[box0], orderedBits(mn));
+                    atomicMax(&c.bs.hmaxBits[cur], orderedBits(m));
+                    atomicMin(&c.bs.hminBits[cur], orderedBits(mn));
+                }
+                cur = -1;
+                m = 0.0;
+                mn = 1e300;
+            };
+            for(int it = 0; it < kHmaxRun; ++it)
+            {
+                uint32_t const g = base + uint32_t(it) * 32u;
+                if(g >= c.n)
+                    break;
+                uint32_t const p = g + uint32_t(lane);
+                int const box = p < c.n ? c.cur.box[p] : -1;
+                double const h = p < c.n ? c.cur.h[p] : 0.0;
+                int const box0 = __shfl_sync(0xffffffffu, box, 0);
+                bool const uniform = __all_sync(0xffffffffu, box == box0 || box < 0);
+                if(uniform && box0 == cur)
+                {
+                    if(box >= 0)
+                    {
+                        m = fmax(m, h);
+                        mn = fmin(mn, h);
+                    }
+                    continue;
+                }
+                flush();
+                if(uniform)
+                {
+                    cur = box0;
+                    if(box >= 0)
+                    {
+                        m = h;
+                        mn = h;
+                    }
+                }
+                else if(box >= 0)
+                {
+                    atomicMax(&c.bs.hmaxBits[box], orderedBits(h));
+                    atomicMin(&c.bs.hminBits[box], orderedBits(h));
                 }
             }
-            else if(box >= 0)
-            {
-                atomicMax(&c.bs.hmaxBits[box], orderedBits(h));
-                atomicMin(&c.bs.hminBits[box], orderedBits(h));
-            }
+            flush();
         }
 
         //! Current grid of every box from its largest h (one block): cell counts
@@ -857,7 +899,8 @@ namespace sph
         cudaMemsetAsync(c.bs.hminBits, 0xff, sizeof(unsigned long long) * c.nbox, s);
         if(c.n)
         {
-            kBoxHmax<<<(c.n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+            uint32_t const perBlock = uint32_t(kThreads / 32) * 32u * uint32_t(kHmaxRun);
+            kBoxHmax<<<(c.n + perBlock - 1) / perBlock, kThreads, 0, s>>>(c);
             countLaunches(1);
         }
         kGrid<<<1, 256, 0, s>>>(c, support);
