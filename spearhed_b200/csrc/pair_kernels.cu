@@ -1323,10 +1323,9 @@ namespace sph
                         A.fold();
                     qc = qn;
                 }
-                // tail: the first n - nFull entries of qc, its first already fetched
                 // the last 1-3 entries (qc.x already fetched); a loop that is not
-                // unrolled keeps one copy of the term, and the fetch after the
-                // last entry re-reads qc.x, a valid entry
+                // unrolled keeps one copy of the pair term, and the fetch after
+                // the last entry re-reads qc.x, a valid entry
                 uint32_t const tail = n - nFull;
 #pragma unroll 1
                 for(uint32_t i = 0; i < tail; ++i)
