@@ -375,6 +375,21 @@ namespace sph
             return mask;
         }
 
+        //! Staged columns are laid out in 32-candidate slabs, each followed by 16
+        //! bytes of padding: the sub-lanes of a short chunk read the same offset
+        //! of different slabs at once, and the skew puts up to eight such slabs
+        //! on different shared-memory banks.  skewed(q) is the column index of
+        //! window position q; a slab's 32 candidates stay contiguous.
+        __device__ __forceinline__ uint32_t skewed(uint32_t q)
+        {
+            return q + ((q >> 5) << 2);
+        }
+        template<int CAP>
+        constexpr int colLen()
+        {
+            return CAP + CAP / 8;
+        }
+
         //! Per-lane state of one chunk of up to 32 targets of a cell.
         template<typename V4, typename T>
         struct TargetChunk
@@ -457,7 +472,8 @@ namespace sph
                 uint32_t mask = 0;
                 if(g < nSlab)
                 {
-                    mask = cullMask32<PAIRMAX, UNR>(ch.own, ch.nR2, sNX + q0, sNY + q0, sNZ + q0, sH + q0, supT, R2g);
+                    uint32_t const c0 = skewed(q0);
+                    mask = cullMask32<PAIRMAX, UNR>(ch.own, ch.nR2, sNX + c0, sNY + c0, sNZ + c0, sH + c0, supT, R2g);
                     if(!ch.act)
                         mask = 0;
                     if(selfq - q0 < 32u)
@@ -663,15 +679,17 @@ namespace sph
             int const lane = threadIdx.x & 31;
             // per warp: negated shifted x, y, z, (pair-max cull) smoothing length, list entry
             constexpr int kCols = PAIRMAX ? 4 : 3;
-            T* const sNX = reinterpret_cast<T*>(smem) + warp * CAP;
-            T* const sNY = sNX + kDensWarps * CAP;
-            T* const sNZ = sNY + kDensWarps * CAP;
-            T* const sH = sNZ + kDensWarps * CAP; // only with PAIRMAX: -(supT h_j)^2
-            uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
+            // (columns in skewed slabs, see skewed())
+            constexpr int kCol = colLen<CAP>();
+            T* const sNX = reinterpret_cast<T*>(smem) + warp * kCol;
+            T* const sNY = sNX + kDensWarps * kCol;
+            T* const sNZ = sNY + kDensWarps * kCol;
+            T* const sH = sNZ + kDensWarps * kCol; // only with PAIRMAX: -(supT h_j)^2
+            uint32_t* const sEnt = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * kCol)
                                    + warp * CAP;
             // per warp: window position of each target's own entry (up to 64
             // targets of the chunk pair; ~0 = not in this window)
-            uint32_t* const sSelf = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * CAP)
+            uint32_t* const sSelf = reinterpret_cast<uint32_t*>(reinterpret_cast<T*>(smem) + kCols * kDensWarps * kCol)
                                     + kDensWarps * CAP + warp * 64;
             Records<V4, T> const rec = records<T>(c);
             T const supT = T(Kern<K>::support);
@@ -970,12 +988,13 @@ namespace sph
                                 if(pass)
                                 {
                                     uint32_t const w = mW + uint32_t(__popc(passMask & ((1u << lane) - 1u)));
-                                    sNX[w] = nx;
-                                    sNY[w] = ny;
-                                    sNZ[w] = nz;
+                                    uint32_t const ws = skewed(w);
+                                    sNX[ws] = nx;
+                                    sNY[ws] = ny;
+                                    sNZ[ws] = nz;
                                     sEnt[w] = ent[k];
                                     if constexpr(PAIRMAX)
-                                        sH[w] = nRj;
+                                        sH[ws] = nRj;
                                     // a target's own entry: centre slot, index among the pair's targets
                                     uint32_t const jr = (ent[k] >> 5) - tc;
                                     if((ent[k] & 31u) == kCentreSlot && jr < nTargets)
@@ -988,11 +1007,12 @@ namespace sph
                         // far candidates up to the next multiple of 32
                         for(uint32_t q = m + uint32_t(lane); q < ((m + 31u) & ~31u); q += 32)
                         {
-                            sNX[q] = T(kFar);
-                            sNY[q] = T(kFar);
-                            sNZ[q] = T(kFar);
+                            uint32_t const qs = skewed(q);
+                            sNX[qs] = T(kFar);
+                            sNY[qs] = T(kFar);
+                            sNZ[qs] = T(kFar);
                             if constexpr(PAIRMAX)
-                                sH[q] = T(0);
+                                sH[qs] = T(0);
                         }
                         __syncwarp();
                         // One copy of the cull serves both chunks (a loop that is not
@@ -1348,7 +1368,8 @@ namespace sph
         template<typename T, bool PM, int CAP>
         constexpr size_t densitySmem()
         {
-            return size_t(kDensWarps) * (CAP * ((PM ? 4 : 3) * sizeof(T) + sizeof(uint32_t)) + 64 * sizeof(uint32_t));
+            return size_t(kDensWarps)
+                   * (colLen<CAP>() * (PM ? 4 : 3) * sizeof(T) + CAP * sizeof(uint32_t) + 64 * sizeof(uint32_t));
         }
 
         // ---- launch-shape variants -------------------------------------------
