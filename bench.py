@@ -19,7 +19,9 @@ value  = accepted ordered pairs per pass x 3 logical pair passes (density,
          (CUDA events on the library's stream), FP32-compensated pair kernels.
 e2e    = the same metric through the C ABI with pinned host buffers: every
          step copies the state in (sph_set_species), runs sph_step(1) and copies
-         the state out (sph_get_species), all inside the timed region.
+         the state out (sph_get_species), all inside the timed region; with N
+         ranks each runs its own boxes between two barriers and the job's time
+         is the slowest rank's.
 fp64_plain = the FP64-plain kernels on the same GPU: the same batched ensemble
          (one context), and the FP64 single-box step looped over the boxes (one
          context per box, the reference's one-simulation-per-run shape); the
@@ -501,8 +503,10 @@ def errors_after_one_step(args, rank, world):
             "bounds": {"density_rel_max": 1e-5, "accel_normwise": 1e-4}}
 
 
-def e2e_leg(args, rank, world, tune, L):
-    """The metric through the C ABI with pinned host buffers: set, step, get."""
+def e2e_leg(args, rank, world, tune, L, barrier=None):
+    """The metric through the C ABI with pinned host buffers: set, step, get.
+    Every rank runs it on its own boxes; the timed loop starts and ends at a
+    barrier, so the slowest rank's time is the job's."""
     import torch
 
     import spearhed_b200 as sb
@@ -537,12 +541,16 @@ def e2e_leg(args, rank, world, tune, L):
     vout.box_id = None
     pe0 = ce.reduce()["pairs_total"]
     torch.cuda.synchronize()
+    if barrier:
+        barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         abi.check(L.sph_set_species(ce._p, 0, abi.ROLES_DEFAULT, host.n, C.byref(vin)))
         abi.check(L.sph_step(ce._p, 1, 0.0))
         abi.check(L.sph_get_species(ce._p, 0, C.byref(vout)))
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if barrier:
+        barrier()
     pe1 = ce.reduce()["pairs_total"]
     ce.close()
     e2e_pairs = (pe1 - pe0) / args.e2e_steps
@@ -669,6 +677,17 @@ def run_ours(args, rank, world):
                           "achieved_with_cull": dens_achieved + cull_achieved,
                           "frac_with_cull": (dens_achieved + cull_achieved) / peak.value if peak.value else None}}
     dominant, other = (dens_info, force_info) if dens_ms >= force_ms else (force_info, dens_info)
+    # ---- end to end through the C ABI with pinned host buffers: every rank on
+    # its own boxes; the job's time is the slowest rank's, pairs and bytes add up
+    e2e_pairs, e2e_s, h2d, d2h = e2e_leg(args, rank, world, tune, L, barrier)
+    if world > 1:
+        import torch.distributed as dist
+        te = torch.tensor([e2e_s, e2e_pairs, h2d, d2h], dtype=torch.float64, device=f"cuda:{dev}")
+        mx = te[0:1].clone()
+        sm = te[1:4].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_pairs, h2d, d2h = float(mx[0]), float(sm[0]), int(sm[1]), int(sm[2])
     result = {}
     if rank != 0:
         return result
@@ -693,8 +712,6 @@ def run_ours(args, rank, world):
     fp64["fp32_speedup"] = fp64.get("box_loop", fp64["batched"])["fp32_speedup"]
     # ---- errors of the FP32 step against the FP64 step from the same state
     errs = errors_after_one_step(args, rank, world)
-    # ---- end to end through the C ABI with pinned host buffers
-    e2e_pairs, e2e_s, h2d, d2h = e2e_leg(args, rank, world, tune, L)
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if world == 1 and not args.no_cpu:
