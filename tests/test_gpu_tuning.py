@@ -26,10 +26,22 @@ def _steps(w, dv, fv, n=3):
     return out
 
 
+# OT: one level, global cull, mostly full chunks.  Rotor and a small Brio-Wu
+# ensemble: two cell levels, the pair-max cull and cells of few targets, so the
+# short chunks' slab cull, the skewed staging slabs and the own-entry positions
+# run in every shape.
+SHAPE_CASES = {
+    "orszag_tang": lambda prec: setups.orszag_tang(nx=32, nz=4, precision=prec, jitter=0.1),
+    "mhd_rotor": lambda prec: setups.mhd_rotor(nxy=64, precision=prec),
+    "brio_wu_ensemble": lambda prec: setups.brio_wu_ensemble(nbox=6, n_lo=4096, n_hi=16384, precision=prec),
+}
+
+
 @pytest.mark.parametrize("prec", [abi.PREC_FP32_COMP, abi.PREC_FP64])
-def test_every_shape_gives_the_same_bits(prec):
+@pytest.mark.parametrize("case", list(SHAPE_CASES))
+def test_every_shape_gives_the_same_bits(prec, case):
     import spearhed_b200 as sb
-    w = setups.orszag_tang(nx=32, nz=4, precision=prec, jitter=0.1)
+    w = SHAPE_CASES[case](prec)
     probe = sb.context_for(w)
     t = probe.tuning()
     probe.close()
