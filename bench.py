@@ -503,6 +503,19 @@ def errors_after_one_step(args, rank, world):
             "bounds": {"density_rel_max": 1e-5, "accel_normwise": 1e-4}}
 
 
+def job_totals(slowest, summed, device):
+    """Whole-job figures from each rank's own, over the default process group:
+    the largest of every value in `slowest` (times: the job ends with its
+    slowest rank) and the sum of every value in `summed` (pairs, bytes)."""
+    import torch
+    import torch.distributed as dist
+    mx = torch.tensor([float(v) for v in slowest], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(v) for v in summed], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return [float(v) for v in mx], [float(v) for v in sm]
+
+
 def e2e_leg(args, rank, world, tune, L, barrier=None):
     """The metric through the C ABI with pinned host buffers: set, step, get.
     Every rank runs it on its own boxes; the timed loop starts and ends at a
@@ -632,12 +645,7 @@ def run_ours(args, rank, world):
     ctx.close()
     ms_total, pairs = r["ms"], r["pairs"]
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_total, pairs], dtype=torch.float64, device=f"cuda:{dev}")
-        mx = t.clone()
-        dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        ms_total, pairs = float(mx[0]), float(t[1])
+        (ms_total,), (pairs,) = job_totals([ms_total], [pairs], f"cuda:{dev}")
     passes = flops.PASSES_PER_STEP[wl_phys]
     value = passes * pairs / (ms_total * 1e-3)
     ms_step = ms_total / args.steps
@@ -681,13 +689,8 @@ def run_ours(args, rank, world):
     # its own boxes; the job's time is the slowest rank's, pairs and bytes add up
     e2e_pairs, e2e_s, h2d, d2h = e2e_leg(args, rank, world, tune, L, barrier)
     if world > 1:
-        import torch.distributed as dist
-        te = torch.tensor([e2e_s, e2e_pairs, h2d, d2h], dtype=torch.float64, device=f"cuda:{dev}")
-        mx = te[0:1].clone()
-        sm = te[1:4].clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_pairs, h2d, d2h = float(mx[0]), float(sm[0]), int(sm[1]), int(sm[2])
+        (e2e_s,), (e2e_pairs, h2d, d2h) = job_totals([e2e_s], [e2e_pairs, h2d, d2h], f"cuda:{dev}")
+        h2d, d2h = int(h2d), int(d2h)
     result = {}
     if rank != 0:
         return result
