@@ -76,6 +76,36 @@ def test_three_in_a_line_density(oracle, prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("cull", [abi.CULL_GLOBAL, abi.CULL_PAIR_MAX])
+@pytest.mark.parametrize("n", [33, 200])
+def test_every_pair_in_reach(oracle, prec, cull, n):
+    """ParticleParticleInteraction.cpp:134-207: with every particle in every
+    other's reach, the accepted pairs are all n(n-1) ordered pairs, self
+    excluded.  n particles in [0.4, 0.6]^3 with h = 0.5 (cull radius 1, above
+    the cloud's diameter) in a non-periodic unit box: one cell holds them all,
+    every acceptance mask is full, and the cell runs full chunks plus a short
+    tail chunk (n = 33: one target on 32 sub-lanes; n = 200: eight targets on
+    four).  The densities are the oracle's."""
+    rng = np.random.default_rng(7)
+    s = abi.Species(n)
+    s.pos[:] = 0.4 + 0.2 * rng.random((3, n))
+    s.mass[:] = 1.0 / n
+    s.h[:] = 0.5
+    p = abi.default_params(precision=prec, h0=0.5, cull=cull)
+    boxes = [abi.make_box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0))]
+    ctx = _ctx(p, boxes, {abi.SPECIES_DEFAULT: s})
+    ctx.density()
+    counts = ctx.neighbour_counts(abi.SPECIES_DEFAULT)
+    rho = ctx.get_species(abi.SPECIES_DEFAULT).density
+    ctx.close()
+    assert np.array_equal(counts, np.full(n, n - 1))
+    orc = _oracle(oracle, p, boxes, {abi.SPECIES_DEFAULT: s})
+    orc.density()
+    rel = np.max(np.abs(rho / orc.s.density - 1.0))
+    assert rel <= TOL[prec]["rho"], rel
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_two_particles_at_rest_repel(oracle, prec):
     d, h = 0.4, 0.5
     s = abi.Species(2)
